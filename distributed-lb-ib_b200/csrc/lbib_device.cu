@@ -1,0 +1,375 @@
+/*
+ * GPU state of one LBM-IB problem and the order of a time step.
+ *
+ * A step (cube_pthread/lbm_ib.c:3124-3563, mpi/do_thread.c:50-386) is
+ *   fiber forces -> spread (node prep, tile compaction, gather) -> fused
+ *   fluid step -> moments on the touched tiles -> interpolate and move
+ * all stream-ordered on one CUDA stream, with no host synchronisation.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "lbib_internal.h"
+
+extern "C" {
+int lbdev_launch_fluid_step(lbib_device* d);
+int lbdev_launch_tile_moments(lbib_device* d);
+int lbdev_launch_field_moments(lbib_device* d, double* rho, double* ux, double* uy, double* uz);
+int lbdev_launch_gather_df1(lbib_device* d, double* out);
+int lbdev_launch_init_eq(lbib_device* d, double* f, long count, long stride);
+int lbdev_launch_fiber_forces(lbib_device* d, int k);
+int lbdev_launch_spread(lbib_device* d, int step);
+int lbdev_launch_move(lbib_device* d);
+int lbdev_launch_scatter_force(lbib_device* d, double* fx, double* fy, double* fz);
+}
+
+#define CK(call)                                  \
+  do {                                            \
+    if ((call) != cudaSuccess) return -2;         \
+  } while (0)
+
+static void free_tiles(lbib_device* d) {
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(d->tile_slot[b]); d->tile_slot[b] = NULL;
+    cudaFree(d->tile_list[b]); d->tile_list[b] = NULL;
+    cudaFree(d->tile_count[b]); d->tile_count[b] = NULL;
+    cudaFree(d->Ftile[b]); d->Ftile[b] = NULL;
+    cudaFree(d->Utile[b]); d->Utile[b] = NULL;
+  }
+  cudaFree(d->tile_flag); d->tile_flag = NULL;
+  cudaFree(d->scan_tmp); d->scan_tmp = NULL;
+}
+
+static void free_sheets(lbib_device* d) {
+  cudaFree(d->nodes); d->nodes = NULL;
+  cudaFree(d->W); d->W = NULL;
+  cudaFree(d->st); d->st = NULL;
+  cudaFree(d->chunk_box); d->chunk_box = NULL;
+  free(d->sh); d->sh = NULL;
+  d->nsheets = 0; d->S = 0; d->nchunks = 0;
+}
+
+/* Collision constants written exactly as the reference evaluates them
+ * (lbm_ib.c:1722-1754): 1 - 1/tau, 1/tau, dt(1 - 1/(2 tau))/w, cs*cs, pow(cs, 4). */
+static void derive_constants(lbib_device* d) {
+  d->omtau = 1.0 - 1.0 / d->tau;
+  d->invtau = 1.0 / d->tau;
+  d->kw[0] = d->dt * (1.0 - 1.0 / (2.0 * d->tau)) / 3.0;
+  d->kw[1] = d->dt * (1.0 - 1.0 / (2.0 * d->tau)) / 18.0;
+  d->kw[2] = d->dt * (1.0 - 1.0 / (2.0 * d->tau)) / 36.0;
+  d->cs2 = d->cs_l * d->cs_l;
+  d->cs4 = pow(d->cs_l, 4);
+  d->half_dt = 0.5 * d->dt;
+  for (int k = 0; k < d->nsheets; ++k) {
+    lbib_sheet_dev* s = &d->sh[k];
+    /* compute_bendingforce / compute_stretchingforce, lbm_ib.c:994-996, 1164-1166, 1230 */
+    s->bc = d->Kb_l / pow(s->ds2, 3);
+    s->sc = d->Ks_l / (s->ds1 * s->ds1);
+    s->sc2 = d->Ks_l / (s->ds2 * s->ds2);
+  }
+}
+
+static void derive_boundaries(lbib_device* d) {
+  /* copy_inout_to_df2 in the serial pthread run reaches z <= ncx*cs - 1 when
+     num_cubes_x < num_cubes_z (lbm_ib.c:2800); otherwise z <= nz - 2. */
+  d->zin_hi = d->nz - 2;
+  if ((d->compat & 4) && d->ncx < d->ncz) d->zin_hi = d->ncx * d->cube_size - 1;
+  /* the y walls skip z rows ncx*cs-2, ncx*cs-1 when num_cubes_x < num_cubes_z
+     (lbm_ib.c:2378, 2414) */
+  d->yskip_z0 = -1;
+  if ((d->compat & 2) && d->ncx < d->ncz) d->yskip_z0 = d->ncx * d->cube_size - 2;
+}
+
+extern "C" int lbdev_set_physics(lbib_device* d, const lbdev_config* c) {
+  d->tau = c->tau; d->u_l = c->u_l; d->rho_l = c->rho_l; d->Ks_l = c->Ks_l; d->Kb_l = c->Kb_l;
+  d->g_l = c->g_l; d->cs_l = c->cs_l; d->dt = c->dt; d->compat = c->compat;
+  derive_constants(d);
+  derive_boundaries(d);
+  return 0;
+}
+
+extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
+  *out = NULL;
+  if (c->nx < 8 || c->ny < 8 || c->nz < 8 || c->cube_size < 4) return -1;
+  if (c->nx % c->cube_size || c->ny % c->cube_size || c->nz % c->cube_size) return -1;
+  lbib_device* d = (lbib_device*)calloc(1, sizeof(lbib_device));
+  if (!d) return -5;
+  d->nx = c->nx; d->ny = c->ny; d->nz = c->nz;
+  d->N = (long)c->nx * c->ny * c->nz;
+  d->cube_size = c->cube_size;
+  d->ncx = c->nx / c->cube_size; d->ncy = c->ny / c->cube_size; d->ncz = c->nz / c->cube_size;
+  lbdev_set_physics(d, c);
+  cudaGetDevice(&d->device);
+  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) { free(d); return -2; }
+  d->ntx = (d->nx + 3) / 4; d->nty = (d->ny + 3) / 4; d->ntz = (d->nz + 3) / 4;
+  d->ntiles = (long)d->ntx * d->nty * d->ntz;
+  int rc = 0;
+  if (cudaMalloc(&d->f, sizeof(double) * 19 * d->N) != cudaSuccess) rc = -5;
+  long P = (long)d->ny * d->nz;
+  if (!rc && cudaMalloc(&d->inlet, sizeof(double) * 19 * P) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&d->outlet, sizeof(double) * 19 * P) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&d->err, sizeof(int) * 2) != cudaSuccess) rc = -5;
+  if (!rc && cudaMallocHost(&d->h_err, sizeof(int) * 2) != cudaSuccess) rc = -5;
+  if (!rc && cudaMemsetAsync(d->err, 0, sizeof(int) * 2, d->stream) != cudaSuccess) rc = -2;
+  if (!rc && cudaMemsetAsync(d->f, 0, sizeof(double) * 19 * d->N, d->stream) != cudaSuccess) rc = -2;
+  if (rc) { lbdev_free(d); return rc; }
+  d->cur = 0;
+  *out = d;
+  return 0;
+}
+
+extern "C" void lbdev_free(lbib_device* d) {
+  if (!d) return;
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  free_tiles(d);
+  free_sheets(d);
+  cudaFree(d->f); cudaFree(d->inlet); cudaFree(d->outlet); cudaFree(d->err);
+  cudaFree(d->scratch);
+  for (long i = 0; i < 6 * d->prof_cap; ++i) cudaEventDestroy(d->prof_ev[i]);
+  free(d->prof_ev);
+  if (d->h_err) cudaFreeHost(d->h_err);
+  if (d->stream) cudaStreamDestroy(d->stream);
+  free(d);
+}
+
+extern "C" int lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_dev* sh, const double* nodes_host) {
+  if (nsheets < 1) return -1;
+  long S = 0;
+  for (int k = 0; k < nsheets; ++k) {
+    if (sh[k].rows < 4 || sh[k].cols < 4) return -1;
+    S += (long)sh[k].rows * sh[k].cols;
+  }
+  CK(cudaStreamSynchronize(d->stream));
+  if (S != d->S) {
+    free_sheets(d);
+    free_tiles(d);
+    d->nchunks = (S + 31) / 32;
+    CK(cudaMalloc(&d->nodes, sizeof(double) * 12 * S));
+    CK(cudaMalloc(&d->W, sizeof(double) * 12 * S));
+    CK(cudaMalloc(&d->st, sizeof(int) * 3 * S));
+    CK(cudaMalloc(&d->chunk_box, sizeof(int) * 6 * d->nchunks));
+    /* every node touches at most 8 tiles, so 8 S slots can never overflow */
+    d->cap = 8 * S < d->ntiles ? 8 * S : d->ntiles;
+    for (int b = 0; b < 2; ++b) {
+      CK(cudaMalloc(&d->tile_slot[b], sizeof(int) * d->ntiles));
+      CK(cudaMalloc(&d->tile_list[b], sizeof(int) * d->cap));
+      CK(cudaMalloc(&d->tile_count[b], sizeof(int)));
+      CK(cudaMalloc(&d->Ftile[b], sizeof(double) * 192 * d->cap));
+      CK(cudaMalloc(&d->Utile[b], sizeof(double) * 256 * d->cap));
+      CK(cudaMemsetAsync(d->tile_slot[b], 0xff, sizeof(int) * d->ntiles, d->stream));
+      CK(cudaMemsetAsync(d->tile_count[b], 0, sizeof(int), d->stream));
+    }
+    CK(cudaMalloc(&d->tile_flag, sizeof(int) * d->ntiles));
+    CK(cudaMalloc(&d->scan_tmp, sizeof(int) * ((d->ntiles + 1023) / 1024 + 1)));
+  }
+  free(d->sh);
+  d->sh = (lbib_sheet_dev*)malloc(sizeof(lbib_sheet_dev) * nsheets);
+  memcpy(d->sh, sh, sizeof(lbib_sheet_dev) * nsheets);
+  long off = 0;
+  for (int k = 0; k < nsheets; ++k) {
+    d->sh[k].offset = off;
+    off += (long)sh[k].rows * sh[k].cols;
+  }
+  d->nsheets = nsheets;
+  d->S = S;
+  derive_constants(d);
+  CK(cudaMemcpyAsync(d->nodes, nodes_host, sizeof(double) * 12 * S, cudaMemcpyHostToDevice, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  d->have_forces = 0;
+  d->have_moments = 0;
+  return 0;
+}
+
+extern "C" int lbdev_init_equilibrium(lbib_device* d) {
+  d->have_eq = 1;
+  return 0;
+}
+
+extern "C" int lbdev_init_df1(lbib_device* d) {
+  if (lbdev_launch_init_eq(d, d->f, d->N, d->N)) return -2;
+  d->parity = 0;
+  d->steps = 0;
+  d->have_df1 = 1;
+  d->have_forces = 0;
+  d->have_moments = 0;
+  for (int b = 0; b < 2; ++b)
+    if (d->tile_slot[b]) CK(cudaMemsetAsync(d->tile_slot[b], 0xff, sizeof(int) * d->ntiles, d->stream));
+  return 0;
+}
+
+extern "C" int lbdev_init_inout(lbib_device* d) {
+  long P = (long)d->ny * d->nz;
+  if (lbdev_launch_init_eq(d, d->inlet, P, P)) return -2;
+  if (lbdev_launch_init_eq(d, d->outlet, P, P)) return -2;
+  d->have_inout = 1;
+  return 0;
+}
+
+extern "C" int lbdev_stage(lbib_device* d, int which, int step_no) {
+  if (!d->nodes || !d->have_df1 || !d->have_inout) return -4;
+  switch (which) {
+    case 0:
+      for (int k = 0; k < d->nsheets; ++k)
+        if (lbdev_launch_fiber_forces(d, k)) return -2;
+      return 0;
+    case 1:
+    case 2:
+      return 0;  /* computed together with the bending force */
+    case 3:
+      d->cur ^= 1;
+      d->have_forces = 1;
+      d->have_moments = 0;
+      return lbdev_launch_spread(d, step_no) ? -2 : 0;
+    case 4:
+      if (!d->have_forces) return -4;
+      return lbdev_launch_fluid_step(d) ? -2 : 0;
+    case 5:
+    case 6:
+      return 0;  /* streaming and bounce-back happen inside the fused step */
+    case 7:
+      d->have_moments = 1;
+      return lbdev_launch_tile_moments(d) ? -2 : 0;
+    case 8:
+      if (!d->have_moments) return -4;
+      return lbdev_launch_move(d) ? -2 : 0;
+    case 9:
+    case 10:
+      return 0;  /* inlet/outlet copy and df2 -> df1 are part of the fused step */
+    default:
+      return -1;
+  }
+}
+
+static int prof_grow(lbib_device* d) {
+  long cap = d->prof_cap ? 2 * d->prof_cap : 256;
+  cudaEvent_t* ev = (cudaEvent_t*)realloc(d->prof_ev, sizeof(cudaEvent_t) * 6 * cap);
+  if (!ev) return -5;
+  d->prof_ev = ev;
+  for (long i = 6 * d->prof_cap; i < 6 * cap; ++i) CK(cudaEventCreate(&d->prof_ev[i]));
+  d->prof_cap = cap;
+  return 0;
+}
+
+extern "C" int lbdev_step(lbib_device* d, int step_no) {
+  static const int order[] = {0, 3, 4, 7, 8};
+  cudaEvent_t* ev = NULL;
+  if (d->profiling) {
+    if (d->prof_steps >= d->prof_cap && prof_grow(d)) return -5;
+    ev = d->prof_ev + 6 * d->prof_steps;
+    CK(cudaEventRecord(ev[0], d->stream));
+  }
+  for (int i = 0; i < 5; ++i) {
+    int rc = lbdev_stage(d, order[i], step_no);
+    if (rc) return rc;
+    if (ev) CK(cudaEventRecord(ev[i + 1], d->stream));
+  }
+  if (ev) d->prof_steps++;
+  return 0;
+}
+
+extern "C" int lbdev_profile_begin(lbib_device* d) {
+  d->profiling = 1;
+  d->prof_steps = 0;
+  return 0;
+}
+
+/* Sums, per stage, the event-timed milliseconds of the steps run since
+ * lbdev_profile_begin, and stops profiling. */
+extern "C" int lbdev_profile_end(lbib_device* d, double* stage_ms, long* steps) {
+  CK(cudaStreamSynchronize(d->stream));
+  for (int s = 0; s < LBIB_NSTAGE_TIMED; ++s) stage_ms[s] = 0.0;
+  for (long t = 0; t < d->prof_steps; ++t) {
+    cudaEvent_t* ev = d->prof_ev + 6 * t;
+    for (int s = 0; s < LBIB_NSTAGE_TIMED; ++s) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev[s], ev[s + 1]));
+      stage_ms[s] += ms;
+    }
+  }
+  if (steps) *steps = d->prof_steps;
+  d->profiling = 0;
+  d->prof_steps = 0;
+  return 0;
+}
+
+extern "C" int lbdev_check(lbib_device* d, int* failed_step) {
+  CK(cudaMemcpyAsync(d->h_err, d->err, sizeof(int) * 2, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  if (failed_step) *failed_step = d->h_err[1];
+  return d->h_err[0];
+}
+
+extern "C" int lbib_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+extern "C" int lbdev_sync(lbib_device* d) {
+  CK(cudaStreamSynchronize(d->stream));
+  return 0;
+}
+
+/* Dense scratch for the getters, allocated per call and freed after it. */
+static int ensure_scratch(lbib_device* d, long doubles) {
+  cudaFree(d->scratch);
+  d->scratch = NULL;
+  CK(cudaMalloc(&d->scratch, sizeof(double) * doubles));
+  return 0;
+}
+
+extern "C" int lbdev_get_moments(lbib_device* d, double* rho, double* ux, double* uy, double* uz) {
+  const long N = d->N;
+  if (ensure_scratch(d, 4 * N)) return -5;
+  double* s = d->scratch;
+  if (lbdev_launch_field_moments(d, s, s + N, s + 2 * N, s + 3 * N)) return -2;
+  CK(cudaMemcpyAsync(rho, s, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaMemcpyAsync(ux, s + N, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaMemcpyAsync(uy, s + 2 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaMemcpyAsync(uz, s + 3 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  cudaFree(d->scratch);
+  d->scratch = NULL;
+  return 0;
+}
+
+extern "C" int lbdev_get_force(lbib_device* d, double* fx, double* fy, double* fz) {
+  const long N = d->N;
+  if (ensure_scratch(d, 3 * N)) return -5;
+  double* s = d->scratch;
+  CK(cudaMemsetAsync(s, 0, sizeof(double) * 3 * N, d->stream));
+  if (d->have_forces && lbdev_launch_scatter_force(d, s, s + N, s + 2 * N)) return -2;
+  CK(cudaMemcpyAsync(fx, s, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaMemcpyAsync(fy, s + N, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaMemcpyAsync(fz, s + 2 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  cudaFree(d->scratch);
+  d->scratch = NULL;
+  return 0;
+}
+
+extern "C" int lbdev_get_df1(lbib_device* d, double* out) {
+  const long N = d->N;
+  if (ensure_scratch(d, 19 * N)) return -5;
+  double* s = d->scratch;
+  CK(cudaMemsetAsync(s, 0, sizeof(double) * 19 * N, d->stream));
+  if (lbdev_launch_gather_df1(d, s)) return -2;
+  CK(cudaMemcpyAsync(out, s, sizeof(double) * 19 * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  cudaFree(d->scratch);
+  d->scratch = NULL;
+  return 0;
+}
+
+extern "C" int lbdev_get_nodes(lbib_device* d, double* out) {
+  CK(cudaMemcpyAsync(out, d->nodes, sizeof(double) * 12 * d->S, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return 0;
+}
+
+extern "C" int lbdev_set_nodes(lbib_device* d, const double* in) {
+  CK(cudaMemcpyAsync(d->nodes, in, sizeof(double) * 12 * d->S, cudaMemcpyHostToDevice, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return 0;
+}

@@ -1,0 +1,406 @@
+/*
+ * Immersed-boundary kernels.
+ *
+ *   lbib_fiber_forces   compute_bendingforce + compute_stretchingforce +
+ *                       compute_elasticforce (cube_pthread/lbm_ib.c:961-1318),
+ *                       one thread per node, both passes of each force in
+ *                       the reference's order.
+ *   lbib_node_prep      per node: stencil start floor(X - 2) + 1 per axis, the
+ *                       twelve delta-kernel factors 1 + cos(pi/2 r) (shared by
+ *                       the spread and the interpolation of the step), the 4^3
+ *                       tiles the stencil touches, and per 32-node chunk the
+ *                       bounding box of its stencils.
+ *   lbib_compact_*      touched tiles -> dense list in tile order and
+ *                       tile -> slot map (deterministic prefix sums).
+ *   lbib_spread_gather  fiber_SpreadForce + fluid_get_SpreadForce
+ *                       (lbm_ib.c:1323-1525) as a gather: one CTA per touched
+ *                       tile, one thread per cell, nodes visited chunk by chunk
+ *                       in global (sheet, row, col) order, so each cell sums
+ *                       its contributions in exactly the reference's order --
+ *                       deterministic, no atomics.
+ *   lbib_move_nodes     moveFiberSheet (lbm_ib.c:2540-2723): one thread per
+ *                       node sums u * w over its 64 stencil cells in the
+ *                       reference's (x, y, z) order, then X += dt U.
+ * All arithmetic keeps the reference's operation order; compile with
+ * -fmad=false.
+ */
+#include "lbib_cos.h"
+#include "lbib_internal.h"
+#include "lbib_lattice.cuh"
+
+namespace {
+
+/* PI as truncated in the reference, cube_pthread/lbm_ib.c:33. */
+constexpr double kPi = 3.14159265358979;
+
+__device__ __forceinline__ void set_error(int* err, int code, int step) {
+  if (atomicCAS(err, 0, code) == 0) err[1] = step;
+}
+
+__global__ void lbib_fiber_forces(double* __restrict__ nodes, int R, int C, double bc, double sc, double sc2,
+                                  double ds1, double ds2, int bend_bug) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R * C) return;
+  const int r = i / C, c = i % C;
+#define P(rr, cc) (nodes + ((long)(rr) * C + (cc)) * 12)
+  const double* m = P(r, c);
+  double b[3], s[3];
+  /* bending along the fiber (row), lbm_ib.c:1002-1052 */
+  for (int d = 0; d < 3; ++d) {
+    if (c == 0) {
+      b[d] = bc * (-P(r, 2)[d] + 2 * P(r, 1)[d] - P(r, 0)[d]);
+    } else if (c == 1) {
+      b[d] = bc * (-P(r, 3)[d] + 4 * P(r, 2)[d] - 5 * P(r, 1)[d] + 2 * P(r, 0)[d]);
+    } else if (c == C - 1) {
+      b[d] = bc * (-P(r, c)[d] + 2 * P(r, c - 1)[d] - P(r, c - 2)[d]);
+    } else if (c == C - 2) {
+      const double last = (d == 0 && bend_bug) ? P(r, c)[d] : P(r, c - 2)[d];
+      b[d] = bc * (2 * P(r, c + 1)[d] - 5 * P(r, c)[d] + 4 * P(r, c - 1)[d] - last);
+    } else {
+      b[d] = bc * (-P(r, c + 2)[d] + 4.0 * P(r, c + 1)[d] - 6.0 * P(r, c)[d] + 4.0 * P(r, c - 1)[d] - P(r, c - 2)[d]);
+    }
+  }
+  /* bending across fibers (column), lbm_ib.c:1062-1145 */
+  for (int d = 0; d < 3; ++d) {
+    double v;
+    if (r == 0) {
+      v = bc * (-P(2, c)[d] + 2 * (P(1, c)[d]) - (P(0, c)[d]));
+    } else if (r == 1) {
+      v = bc * (-P(3, c)[d] + 4 * (P(2, c)[d]) - 5 * (P(1, c)[d]) + 2 * (P(0, c)[d]));
+    } else if (r == R - 1) {
+      v = bc * (-(P(r, c)[d]) + 2 * (P(r - 1, c)[d]) - (P(r - 2, c)[d]));
+    } else if (r == R - 2) {
+      v = bc * (2 * P(r + 1, c)[d] - 5 * (P(r, c)[d]) + 4 * (P(r - 1, c)[d]) - (P(r - 2, c)[d]));
+    } else {
+      v = bc * (-P(r + 2, c)[d] + 4.0 * (P(r + 1, c)[d]) - 6.0 * (P(r, c)[d]) + 4.0 * (P(r - 1, c)[d]) - (P(r - 2, c)[d]));
+    }
+    b[d] = b[d] + v;
+  }
+  /* stretching along the fiber (row), lbm_ib.c:1179-1221 */
+  if (c == 0) {
+    const double* p = P(r, 1);
+    const double t0 = p[0] - m[0], t1 = p[1] - m[1], t2 = p[2] - m[2];
+    const double dr = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+    s[0] = sc * ((dr - ds1) * (t0 / dr));
+    s[1] = sc * ((dr - ds1) * (t1 / dr));
+    s[2] = sc * ((dr - ds1) * (t2 / dr));
+  } else if (c == C - 1) {
+    const double* q = P(r, C - 2);
+    const double t0 = m[0] - q[0], t1 = m[1] - q[1], t2 = m[2] - q[2];
+    const double dl = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+    s[0] = sc * ((dl - ds1) * (t0 / dl));
+    s[1] = sc * ((dl - ds1) * (t1 / dl));
+    s[2] = sc * ((dl - ds1) * (t2 / dl));
+  } else {
+    const double* p = P(r, c + 1);
+    const double* q = P(r, c - 1);
+    const double r0 = p[0] - m[0], r1 = p[1] - m[1], r2 = p[2] - m[2];
+    const double l0 = q[0] - m[0], l1 = q[1] - m[1], l2 = q[2] - m[2];
+    const double dr = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
+    const double dl = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
+    s[0] = sc * ((dr - ds1) * (r0 / dr) + (dl - ds1) * (l0 / dl));
+    s[1] = sc * ((dr - ds1) * (r1 / dr) + (dl - ds1) * (l1 / dl));
+    s[2] = sc * ((dr - ds1) * (r2 / dr) + (dl - ds1) * (l2 / dl));
+  }
+  /* stretching across fibers (column), lbm_ib.c:1233-1278 */
+  if (r == 0) {
+    const double* p = P(1, c);
+    const double t0 = p[0] - m[0], t1 = p[1] - m[1], t2 = p[2] - m[2];
+    const double dt = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+    s[0] = s[0] + sc2 * ((dt - ds2) * (t0 / dt));
+    s[1] = s[1] + sc2 * ((dt - ds2) * (t1 / dt));
+    s[2] = s[2] + sc2 * ((dt - ds2) * (t2 / dt));
+  } else if (r == R - 1) {
+    const double* q = P(R - 2, c);
+    const double t0 = m[0] - q[0], t1 = m[1] - q[1], t2 = m[2] - q[2];
+    const double db = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+    s[0] = s[0] + sc2 * ((db - ds2) * (t0 / db));
+    s[1] = s[1] + sc2 * ((db - ds2) * (t1 / db));
+    s[2] = s[2] + sc2 * ((db - ds2) * (t2 / db));
+  } else {
+    const double* p = P(r + 1, c);
+    const double* q = P(r - 1, c);
+    const double a0 = p[0] - m[0], a1 = p[1] - m[1], a2 = p[2] - m[2];
+    const double e0 = q[0] - m[0], e1 = q[1] - m[1], e2 = q[2] - m[2];
+    const double dt = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+    const double db = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+    s[0] = s[0] + sc2 * ((dt - ds2) * (a0 / dt) + (db - ds2) * (e0 / db));
+    s[1] = s[1] + sc2 * ((dt - ds2) * (a1 / dt) + (db - ds2) * (e1 / db));
+    s[2] = s[2] + sc2 * ((dt - ds2) * (a2 / dt) + (db - ds2) * (e2 / db));
+  }
+#undef P
+  double* o = nodes + (long)i * 12;
+  o[3] = b[0]; o[4] = b[1]; o[5] = b[2];
+  o[6] = s[0]; o[7] = s[1]; o[8] = s[2];
+  /* compute_elasticforce, lbm_ib.c:1303-1308: stretch + bend */
+  o[9] = s[0] + b[0]; o[10] = s[1] + b[1]; o[11] = s[2] + b[2];
+}
+
+__device__ __forceinline__ int stencil_start(double p) { return (int)(floor(p / 1.0 - 2) + 1); }
+
+__global__ void lbib_node_prep(const double* __restrict__ nodes, long S, int nx, int ny, int nz, int ntx, int nty,
+                               double* __restrict__ W, int* __restrict__ st, int* __restrict__ tile_flag,
+                               int* __restrict__ chunk_box, int* err, int step) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  int b0 = INT_MAX, b1 = INT_MIN, b2 = INT_MAX, b3 = INT_MIN, b4 = INT_MAX, b5 = INT_MIN;
+  if (i < S) {
+    const double* m = nodes + i * 12;
+    const int is = stencil_start(m[0]), js = stencil_start(m[1]), ks = stencil_start(m[2]);
+    st[i * 3 + 0] = is; st[i * 3 + 1] = js; st[i * 3 + 2] = ks;
+    const double cxk = kPi / (2.0 * 1.0);
+    double* w = W + i * 12;
+    for (int a = 0; a < 4; ++a) {
+      w[a] = 1.0e0 + lbib_cos(cxk * (1.0 * (is + a) - m[0]));
+      w[4 + a] = 1.0e0 + lbib_cos(cxk * (1.0 * (js + a) - m[1]));
+      w[8 + a] = 1.0e0 + lbib_cos(cxk * (1.0 * (ks + a) - m[2]));
+    }
+    if (is < 0 || is + 3 >= nx || js < 0 || js + 3 >= ny || ks < 0 || ks + 3 >= nz) {
+      set_error(err, -3, step);
+    } else {
+      for (int tz = ks >> 2; tz <= (ks + 3) >> 2; ++tz)
+        for (int ty = js >> 2; ty <= (js + 3) >> 2; ++ty)
+          for (int tx = is >> 2; tx <= (is + 3) >> 2; ++tx) tile_flag[((long)tz * nty + ty) * ntx + tx] = 1;
+      b0 = is; b1 = is + 3; b2 = js; b3 = js + 3; b4 = ks; b5 = ks + 3;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    b0 = min(b0, __shfl_xor_sync(0xffffffffu, b0, o));
+    b1 = max(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+    b2 = min(b2, __shfl_xor_sync(0xffffffffu, b2, o));
+    b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, o));
+    b4 = min(b4, __shfl_xor_sync(0xffffffffu, b4, o));
+    b5 = max(b5, __shfl_xor_sync(0xffffffffu, b5, o));
+  }
+  const long chunk = i >> 5;
+  if (lane == 0 && chunk * 32 < S) {
+    int* bx = chunk_box + chunk * 6;
+    bx[0] = b0; bx[1] = b1; bx[2] = b2; bx[3] = b3; bx[4] = b4; bx[5] = b5;
+  }
+}
+
+/* Deterministic compaction of tile_flag: per-block counts, one-block scan,
+ * then each block writes its touched tiles in index order. */
+constexpr int kScanBlock = 1024;
+
+__global__ void lbib_compact_count(const int* __restrict__ flag, long n, int* __restrict__ block_sum) {
+  __shared__ int s[32];
+  const long i = (long)blockIdx.x * kScanBlock + threadIdx.x;
+  int v = (i < n) ? (flag[i] != 0) : 0;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int w = s[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+    if (threadIdx.x == 0) block_sum[blockIdx.x] = w;
+  }
+}
+
+__global__ void lbib_compact_scan(int* __restrict__ block_sum, int nblocks, int* __restrict__ total) {
+  __shared__ int s[kScanBlock];
+  int carry = 0;
+  for (int base = 0; base < nblocks; base += kScanBlock) {
+    const int i = base + threadIdx.x;
+    const int v = (i < nblocks) ? block_sum[i] : 0;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < kScanBlock; o <<= 1) {
+      const int t = (threadIdx.x >= (unsigned)o) ? s[threadIdx.x - o] : 0;
+      __syncthreads();
+      s[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < nblocks) block_sum[i] = carry + s[threadIdx.x] - v;
+    const int last = s[kScanBlock - 1];
+    __syncthreads();
+    carry += last;
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void lbib_compact_write(const int* __restrict__ flag, long n, const int* __restrict__ block_off,
+                                   int* __restrict__ list, int* __restrict__ slot) {
+  __shared__ int s[32];
+  const long i = (long)blockIdx.x * kScanBlock + threadIdx.x;
+  const int v = (i < n) ? (flag[i] != 0) : 0;
+  const unsigned bal = __ballot_sync(0xffffffffu, v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) s[warp] = __popc(bal);
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int w = s[threadIdx.x];
+    int incl = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    s[threadIdx.x] = incl - w;
+  }
+  __syncthreads();
+  if (v) {
+    const int pos = block_off[blockIdx.x] + s[warp] + __popc(bal & ((1u << lane) - 1u));
+    list[pos] = (int)i;
+    slot[i] = pos;
+  }
+}
+
+/* One CTA (64 threads = one 4^3 tile) per touched tile. */
+__global__ void __launch_bounds__(64) lbib_spread_gather(const double* __restrict__ nodes, const double* __restrict__ W,
+                                                         const int* __restrict__ st, const int* __restrict__ chunk_box,
+                                                         long S, long nchunks, const int* __restrict__ list,
+                                                         const int* __restrict__ count, int ntx, int nty,
+                                                         double* __restrict__ Ftile, const int* err) {
+  __shared__ int hit[64];
+  __shared__ int s_st[32][3];
+  __shared__ double s_w[32][12];
+  __shared__ double s_fe[32][3];
+  if (*(volatile const int*)err) return;
+  const int n = *count;
+  const int cell = threadIdx.x;
+  const double cf = 1.0 / (64.0 * 1.0 * 1.0 * 1.0);
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const int tile = list[it];
+    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+    const int x0 = tx * 4, y0 = ty * 4, z0 = tz * 4;
+    const int gx = x0 + (cell & 3), gy = y0 + ((cell >> 2) & 3), gz = z0 + (cell >> 4);
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    for (long c0 = 0; c0 < nchunks; c0 += 64) {
+      const long c = c0 + cell;
+      int h = 0;
+      if (c < nchunks) {
+        const int* bx = chunk_box + c * 6;
+        h = !(bx[1] < x0 || bx[0] > x0 + 3 || bx[3] < y0 || bx[2] > y0 + 3 || bx[5] < z0 || bx[4] > z0 + 3);
+      }
+      __syncthreads();
+      hit[cell] = h;
+      __syncthreads();
+      for (int k = 0; k < 64; ++k) {
+        if (!hit[k]) continue;
+        const long base = (c0 + k) * 32;
+        if (cell < 32) {
+          const long nd = base + cell;
+          if (nd < S) {
+            s_st[cell][0] = st[nd * 3 + 0]; s_st[cell][1] = st[nd * 3 + 1]; s_st[cell][2] = st[nd * 3 + 2];
+            for (int a = 0; a < 12; ++a) s_w[cell][a] = W[nd * 12 + a];
+            s_fe[cell][0] = nodes[nd * 12 + 9]; s_fe[cell][1] = nodes[nd * 12 + 10]; s_fe[cell][2] = nodes[nd * 12 + 11];
+          } else {
+            s_st[cell][0] = INT_MIN / 2; s_st[cell][1] = INT_MIN / 2; s_st[cell][2] = INT_MIN / 2;
+          }
+        }
+        __syncthreads();
+        for (int j = 0; j < 32; ++j) {
+          const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
+          if ((unsigned)a < 4u && (unsigned)b < 4u && (unsigned)e < 4u) {
+            const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
+            Fx = Fx + s_fe[j][0] * tmp;
+            Fy = Fy + s_fe[j][1] * tmp;
+            Fz = Fz + s_fe[j][2] * tmp;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    double* Ft = Ftile + (long)it * 192;
+    Ft[cell] = Fx; Ft[64 + cell] = Fy; Ft[128 + cell] = Fz;
+  }
+}
+
+__global__ void lbib_move_nodes(double* __restrict__ nodes, const double* __restrict__ W, const int* __restrict__ st,
+                                long S, int ntx, int nty, const int* __restrict__ slot, const double* __restrict__ Utile,
+                                double dt, const int* err) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S) return;
+  if (*(volatile const int*)err) return;
+  const double c_64 = 1.0 / (6.4e1);
+  const int is = st[i * 3 + 0], js = st[i * 3 + 1], ks = st[i * 3 + 2];
+  const double* w = W + i * 12;
+  double s1 = 0, s2 = 0, s3 = 0;
+  for (int i2 = 0; i2 <= 3; i2++) {
+    const int gi = is + i2;
+    for (int j2 = 0; j2 <= 3; j2++) {
+      const int gj = js + j2;
+      for (int k2 = 0; k2 <= 3; k2++) {
+        const int gk = ks + k2;
+        const int sp = slot[lbib::tile_of(gi, gj, gk, ntx, nty)];
+        const double* U = Utile + (long)sp * 256;
+        const int cell = lbib::cell_in_tile(gi, gj, gk);
+        const double vx = U[64 + cell], vy = U[128 + cell], vz = U[192 + cell];
+        s1 += vx * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
+        s2 += vy * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
+        s3 += vz * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
+      }
+    }
+  }
+  double* m = nodes + i * 12;
+  m[0] += dt * s1;
+  m[1] += dt * s2;
+  m[2] += dt * s3;
+}
+
+/* Dense copy of the spread force for getters: zero, then each touched tile. */
+__global__ void lbib_scatter_force(const int* __restrict__ list, const int* __restrict__ count,
+                                   const double* __restrict__ Ftile, int nx, int ny, int nz, int ntx, int nty,
+                                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+  const int n = *count;
+  const int cell = threadIdx.x;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const int tile = list[it];
+    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+    const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
+    if (x < nx && y < ny && z < nz) {
+      const long idx = ((long)z * ny + y) * nx + x;
+      const double* Ft = Ftile + (long)it * 192;
+      fx[idx] = Ft[cell]; fy[idx] = Ft[64 + cell]; fz[idx] = Ft[128 + cell];
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int lbdev_launch_fiber_forces(lbib_device* d, int k) {
+  const lbib_sheet_dev* s = &d->sh[k];
+  const int n = s->rows * s->cols;
+  lbib_fiber_forces<<<(n + 127) / 128, 128, 0, d->stream>>>(d->nodes + s->offset * 12, s->rows, s->cols, s->bc,
+                                                            s->sc, s->sc2, s->ds1, s->ds2,
+                                                            (d->compat & 1) != 0);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
+  const int c = d->cur;
+  cudaStream_t st = d->stream;
+  if (cudaMemsetAsync(d->tile_flag, 0, d->ntiles * sizeof(int), st) != cudaSuccess) return -2;
+  if (cudaMemsetAsync(d->tile_slot[c], 0xff, d->ntiles * sizeof(int), st) != cudaSuccess) return -2;
+  const long S = d->S;
+  const unsigned nb = (unsigned)((S + 127) / 128);
+  lbib_node_prep<<<nb, 128, 0, st>>>(d->nodes, S, d->nx, d->ny, d->nz, d->ntx, d->nty, d->W, d->st, d->tile_flag,
+                                     d->chunk_box, d->err, step);
+  const unsigned nblk = (unsigned)((d->ntiles + kScanBlock - 1) / kScanBlock);
+  lbib_compact_count<<<nblk, kScanBlock, 0, st>>>(d->tile_flag, d->ntiles, d->scan_tmp);
+  lbib_compact_scan<<<1, kScanBlock, 0, st>>>(d->scan_tmp, (int)nblk, d->tile_count[c]);
+  lbib_compact_write<<<nblk, kScanBlock, 0, st>>>(d->tile_flag, d->ntiles, d->scan_tmp, d->tile_list[c],
+                                                  d->tile_slot[c]);
+  lbib_spread_gather<<<148 * 8, 64, 0, st>>>(d->nodes, d->W, d->st, d->chunk_box, S, d->nchunks, d->tile_list[c],
+                                             d->tile_count[c], d->ntx, d->nty, d->Ftile[c], d->err);
+  d->kernel_launches += 5;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+extern "C" int lbdev_launch_move(lbib_device* d) {
+  const int c = d->cur;
+  const unsigned nb = (unsigned)((d->S + 127) / 128);
+  lbib_move_nodes<<<nb, 128, 0, d->stream>>>(d->nodes, d->W, d->st, d->S, d->ntx, d->nty, d->tile_slot[c],
+                                             d->Utile[c], (double)d->dt, d->err);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+extern "C" int lbdev_launch_scatter_force(lbib_device* d, double* fx, double* fy, double* fz) {
+  const int c = d->cur;
+  lbib_scatter_force<<<148 * 8, 64, 0, d->stream>>>(d->tile_list[c], d->tile_count[c], d->Ftile[c], d->nx, d->ny,
+                                                     d->nz, d->ntx, d->nty, fx, fy, fz);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}

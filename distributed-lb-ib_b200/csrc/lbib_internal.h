@@ -1,0 +1,125 @@
+/*
+ * Internal interface between the host C layer (lbib_api.c) and the CUDA
+ * translation units.  Not installed; include/lbib.h is the public ABI.
+ *
+ * GPU data layout (one fluid grid, several sheets):
+ *   f        [19][N] FP64 populations, N = nx*ny*nz, idx = (z*ny + y)*nx + x.
+ *            One buffer, updated in place with the AA access pattern; `parity`
+ *            says how the next fused step must read it (0: each cell's own
+ *            slots in natural order; 1: the neighbours' opposite slots).
+ *   inlet/outlet [19][ny*nz] fixed equilibria (reference df_inout planes).
+ *   tiles    the grid is cut into 4x4x4 tiles; a step's force spread touches
+ *            few of them.  For the current and the previous step the library
+ *            keeps tile -> slot maps and per-slot arrays: force F(t) [slot][3][64]
+ *            and moments (rho, u)(t) [slot][4][64].
+ *   nodes    [S][12] Fibernode records of all sheets, concatenated.
+ *   weights  [S][12] the delta-kernel factors (1 + cos(pi/2 r)) of each node's
+ *            4x4x4 stencil (4 per axis), and [S][3] its start indices.
+ */
+#ifndef LBIB_INTERNAL_H
+#define LBIB_INTERNAL_H
+
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBIB_TILE 4
+#define LBIB_TILE_CELLS 64
+#define LBIB_CHUNK 32
+
+typedef struct lbib_sheet_dev {
+  int rows, cols;
+  long offset;                   /* first node in the concatenated arrays */
+  double bc;                     /* Kb_l / ds2^3                  (bending)    */
+  double sc, sc2;                /* Ks_l / ds1^2, Ks_l / ds2^2    (stretching) */
+  double ds1, ds2;               /* width/(cols-1), height/(rows-1)            */
+} lbib_sheet_dev;
+
+typedef struct lbib_device {
+  int nx, ny, nz;
+  long N;
+  int cube_size, ncx, ncy, ncz;
+  int compat;
+  int zin_hi;                    /* last z row the inlet/outlet copy reaches  */
+  int yskip_z0;                  /* y walls skip rows z0, z0+1 (or -1)        */
+  /* physics and the collision constants, computed on the host exactly as the
+     reference writes them */
+  double tau, u_l, rho_l, Ks_l, Kb_l, g_l, cs_l;
+  int dt;
+  double omtau, invtau, kw[3], cs2, cs4, half_dt;
+  /* populations */
+  double* f;
+  double* inlet;
+  double* outlet;
+  int parity;
+  long steps;                    /* fused steps since init_df1               */
+  int have_eq, have_df1, have_inout;
+  /* force / moment tiles, double buffered by step */
+  int ntx, nty, ntz;
+  long ntiles;
+  long cap;                      /* slots per buffer                          */
+  int* tile_flag;                /* [ntiles] scratch                          */
+  int* tile_slot[2];             /* [ntiles] slot or -1                       */
+  int* tile_list[2];             /* [cap] touched tiles in index order        */
+  int* tile_count[2];            /* [1]                                       */
+  int* scan_tmp;                 /* block sums for the compaction             */
+  double* Ftile[2];              /* [cap][3][64]                              */
+  double* Utile[2];              /* [cap][4][64]                              */
+  int cur;                       /* buffers of the step in progress / last    */
+  int have_forces;               /* Ftile[cur] holds this step's spread       */
+  int have_moments;              /* Utile[cur] holds this step's moments      */
+  /* sheets */
+  int nsheets;
+  long S;
+  lbib_sheet_dev* sh;            /* host array [nsheets]                      */
+  double* nodes;                 /* [S][12]                                   */
+  double* W;                     /* [S][12]                                   */
+  int* st;                       /* [S][3]                                    */
+  int* chunk_box;                /* [nchunks][6]                              */
+  long nchunks;
+  /* errors and plumbing */
+  int* err;                      /* [2]: code, step                           */
+  int* h_err;                    /* pinned mirror                             */
+  double* scratch;               /* dense field scratch for getters           */
+  cudaStream_t stream;
+  int device;
+  long kernel_launches;          /* kernels this state has launched           */
+  /* optional stage timing: events around the five stages of each step */
+  int profiling;
+  cudaEvent_t* prof_ev;          /* [prof_cap][6]                             */
+  long prof_steps, prof_cap;
+} lbib_device;
+
+#define LBIB_NSTAGE_TIMED 5      /* forces, spread, fluid, moments, move */
+
+typedef struct lbdev_config {
+  int nx, ny, nz, cube_size, compat;
+  double tau, u_l, rho_l, Ks_l, Kb_l, g_l, cs_l;
+  int dt;
+} lbdev_config;
+
+int  lbdev_create(lbib_device** out, const lbdev_config* cfg);
+void lbdev_free(lbib_device* d);
+int  lbdev_set_physics(lbib_device* d, const lbdev_config* cfg);
+int  lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_dev* sh, const double* nodes_host);
+int  lbdev_init_equilibrium(lbib_device* d);   /* init_eqlbrmdistrfuncDF0 */
+int  lbdev_init_df1(lbib_device* d);           /* init_df1 */
+int  lbdev_init_inout(lbib_device* d);         /* init_df_inout */
+int  lbdev_stage(lbib_device* d, int which, int step_no);
+int  lbdev_step(lbib_device* d, int step_no);
+int  lbdev_check(lbib_device* d, int* failed_step);  /* syncs, reads error word */
+int  lbdev_get_moments(lbib_device* d, double* rho, double* ux, double* uy, double* uz);
+int  lbdev_get_force(lbib_device* d, double* fx, double* fy, double* fz);
+int  lbdev_get_df1(lbib_device* d, double* out);
+int  lbdev_get_nodes(lbib_device* d, double* out);
+int  lbdev_set_nodes(lbib_device* d, const double* in);
+int  lbdev_sync(lbib_device* d);
+int  lbdev_profile_begin(lbib_device* d);
+int  lbdev_profile_end(lbib_device* d, double* stage_ms, long* steps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,223 @@
+"""Python binding of liblbib.so (include/lbib.h) for tests, tools and bench.py.
+
+The solver runs on the GPU through the C ABI only; there is no CPU path.
+Loading fails loudly when the library is missing or was built for another
+architecture.  Field arrays are x-fastest (``idx = (z*ny + y)*nx + x``) and
+returned shaped (nz, ny, nx); sheet records are the reference's Fibernode
+(12 doubles: x y z, bend xyz, stretch xyz, elastic xyz), shaped (rows, cols, 12).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbib.so")
+
+COMPAT_BEND_X_BUG = 1
+COMPAT_YWALL_CUBES_X = 2
+COMPAT_INOUT_PTHREAD = 4
+COMPAT_ALL = 7
+
+DUMP_NONE = 0
+DUMP_FIELDVIEW = 1
+DUMP_BINARY = 2
+
+STAGES = {"bending": 0, "stretching": 1, "elastic": 2, "spread": 3, "collide": 4, "stream": 5,
+          "bounceback": 6, "moments": 7, "move": 8, "copy_inout": 9, "replace": 10}
+
+EXPORTED = [
+    "init_gv_constant", "gen_fluid_grid", "gen_fiber_sheet", "init_gv", "init_eqlbrmdistrfuncDF0",
+    "init_df1", "init_df_inout", "do_thread", "compute_bendingforce", "compute_stretchingforce",
+    "compute_elasticforce", "fiber_SpreadForce", "fluid_get_SpreadForce",
+    "get_influentialdomain_fluid_grid_and_SpreadForce", "compute_eqlbrmdistrfuncDF1", "stream_distrfunc",
+    "bounceback_rigidwalls", "compute_rho_and_u", "fluid_SpreadVelocity", "fiber_get_SpreadVelocity",
+    "moveFiberSheet", "copy_inout_to_df2", "replace_old_DF", "periodicBC", "save_fiber_sub_grid",
+    "save_fiber_sub_grid_binary", "save_fluid_sub_grid", "save_fluid_sub_grid_vel_use_fv",
+    "save_fluid_sub_grid_cord_use_fv", "save_fiber_sub_grid_cord_ef_use_fv", "lbib_set_params",
+    "lbib_set_compat", "lbib_last_error", "lbib_error_string", "lbib_clear_error", "lbib_sync_to_host",
+    "lbib_free", "lbib_get_moments", "lbib_get_force", "lbib_get_df1", "lbib_get_sheet", "lbib_set_sheet",
+    "lbib_run", "lbib_synchronize", "lbib_stream", "lbib_case_create", "lbib_case_free", "lbib_stage",
+    "lbib_device_count", "lbib_kernel_launches", "lbib_profile_begin", "lbib_profile_end",
+]
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lib: Optional[C.CDLL] = None
+
+
+class LbibError(RuntimeError):
+    pass
+
+
+def build(quiet: bool = True) -> str:
+    """Compile liblbib.so in place (nvcc, sm_100a)."""
+    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise LbibError("liblbib build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])
+    if not quiet:
+        print(out.stdout)
+    return LIB_PATH
+
+
+def load() -> C.CDLL:
+    """Load liblbib.so and declare the C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise LbibError(f"{LIB_PATH} is missing; build it with `make -C {HERE}`")
+    lib = C.CDLL(LIB_PATH)
+    lib.lbib_case_create.restype = C.c_void_p
+    lib.lbib_case_create.argtypes = [C.c_int] * 5 + [_ip, _ip] + [_dp] * 5 + [C.c_double] * 4 + [C.c_int]
+    lib.lbib_case_free.argtypes = [C.c_void_p]
+    lib.lbib_case_free.restype = None
+    lib.lbib_run.argtypes = [C.c_void_p, C.c_int]
+    lib.lbib_stage.argtypes = [C.c_void_p, C.c_int]
+    for n in ["lbib_get_moments"]:
+        getattr(lib, n).argtypes = [C.c_void_p] + [_dp] * 4
+    lib.lbib_get_force.argtypes = [C.c_void_p] + [_dp] * 3
+    lib.lbib_get_df1.argtypes = [C.c_void_p, _dp]
+    lib.lbib_get_sheet.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.lbib_set_sheet.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.lbib_synchronize.argtypes = [C.c_void_p]
+    lib.lbib_stream.argtypes = [C.c_void_p]
+    lib.lbib_stream.restype = C.c_void_p
+    lib.lbib_last_error.restype = C.c_int
+    lib.lbib_error_string.argtypes = [C.c_int]
+    lib.lbib_error_string.restype = C.c_char_p
+    lib.lbib_clear_error.restype = None
+    lib.lbib_set_compat.argtypes = [C.c_void_p, C.c_int]
+    lib.lbib_set_params.argtypes = [C.c_void_p] + [C.c_double] * 4
+    lib.lbib_device_count.restype = C.c_int
+    lib.lbib_kernel_launches.argtypes = [C.c_void_p]
+    lib.lbib_kernel_launches.restype = C.c_long
+    lib.lbib_profile_begin.argtypes = [C.c_void_p]
+    lib.lbib_profile_end.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_long)]
+    for n in ["init_gv_constant", "init_gv", "init_eqlbrmdistrfuncDF0", "init_df1", "init_df_inout",
+              "lbib_free"]:
+        getattr(lib, n).argtypes = [C.c_void_p]
+        getattr(lib, n).restype = None
+    lib.lbib_sync_to_host.argtypes = [C.c_void_p]
+    lib.do_thread.argtypes = [C.c_void_p]
+    lib.do_thread.restype = C.c_void_p
+    _lib = lib
+    return lib
+
+
+def device_count() -> int:
+    return load().lbib_device_count()
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = load().lbib_error_string(rc).decode()
+        load().lbib_clear_error()
+        raise LbibError(f"{what}: {msg} ({rc})")
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class Solver:
+    """One LBM-IB problem on the GPU, set up through the reference-named API.
+
+    ``case`` is any object with ``nx, ny, nz, cube_size, tau, u_l, Ks_l, Kb_l,
+    compat`` and ``sheets`` (each with ``rows, cols, width, height, x0, y0,
+    z0``), in the reference's internal axes (x = flow direction).
+    """
+
+    def __init__(self, case):
+        lib = load()
+        self.lib = lib
+        self.case = case
+        sh: Sequence = case.sheets
+        k = len(sh)
+        ia = lambda v: (C.c_int * k)(*v)
+        da = lambda v: (C.c_double * k)(*v)
+        lib.lbib_clear_error()
+        self.gv = lib.lbib_case_create(
+            case.nx, case.ny, case.nz, case.cube_size, k,
+            ia([s.rows for s in sh]), ia([s.cols for s in sh]),
+            da([s.width for s in sh]), da([s.height for s in sh]),
+            da([s.x0 for s in sh]), da([s.y0 for s in sh]), da([s.z0 for s in sh]),
+            case.tau, case.u_l, case.Ks_l, case.Kb_l, case.compat)
+        if not self.gv:
+            rc = lib.lbib_last_error()
+            lib.lbib_clear_error()
+            raise LbibError(f"lbib_case_create failed: {lib.lbib_error_string(rc).decode()} ({rc})")
+        self.N = case.nx * case.ny * case.nz
+
+    def close(self) -> None:
+        if getattr(self, "gv", None):
+            self.lib.lbib_case_free(self.gv)
+            self.gv = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def run(self, nsteps: int) -> None:
+        _check(self.lib.lbib_run(self.gv, nsteps), "lbib_run")
+
+    def stage(self, name: str) -> None:
+        _check(self.lib.lbib_stage(self.gv, STAGES[name]), "lbib_stage " + name)
+
+    def synchronize(self) -> None:
+        _check(self.lib.lbib_synchronize(self.gv), "lbib_synchronize")
+
+    @property
+    def stream(self) -> int:
+        return self.lib.lbib_stream(self.gv) or 0
+
+    @property
+    def kernel_launches(self) -> int:
+        return self.lib.lbib_kernel_launches(self.gv)
+
+    def profile_begin(self) -> None:
+        _check(self.lib.lbib_profile_begin(self.gv), "lbib_profile_begin")
+
+    def profile_end(self):
+        """Summed ms per stage (forces, spread, fluid, moments, move), steps."""
+        ms = np.zeros(5)
+        n = C.c_long(0)
+        _check(self.lib.lbib_profile_end(self.gv, _ptr(ms), C.byref(n)), "lbib_profile_end")
+        return dict(zip(["forces", "spread", "fluid", "moments", "move"], ms.tolist())), n.value
+
+    def moments(self):
+        c = self.case
+        a = [np.empty(self.N) for _ in range(4)]
+        _check(self.lib.lbib_get_moments(self.gv, *[_ptr(x) for x in a]), "lbib_get_moments")
+        return [x.reshape(c.nz, c.ny, c.nx) for x in a]
+
+    def force(self):
+        c = self.case
+        a = [np.empty(self.N) for _ in range(3)]
+        _check(self.lib.lbib_get_force(self.gv, *[_ptr(x) for x in a]), "lbib_get_force")
+        return [x.reshape(c.nz, c.ny, c.nx) for x in a]
+
+    def df1(self) -> np.ndarray:
+        c = self.case
+        a = np.empty(19 * self.N)
+        _check(self.lib.lbib_get_df1(self.gv, _ptr(a)), "lbib_get_df1")
+        return a.reshape(19, c.nz, c.ny, c.nx)
+
+    def sheet(self, k: int = 0) -> np.ndarray:
+        s = self.case.sheets[k]
+        a = np.empty(s.rows * s.cols * 12)
+        _check(self.lib.lbib_get_sheet(self.gv, k, _ptr(a)), "lbib_get_sheet")
+        return a.reshape(s.rows, s.cols, 12)
+
+    def set_sheet(self, k: int, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+        _check(self.lib.lbib_set_sheet(self.gv, k, _ptr(a)), "lbib_set_sheet")

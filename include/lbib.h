@@ -1,0 +1,296 @@
+/*
+ * lbib.h -- drop-in C ABI for the LBM-IB time-step loop of
+ * IUPU-HPC/distributed-LB-IB, executed on one NVIDIA B200 (sm_100a).
+ *
+ * A host program written against the reference (mpi/main.c, or
+ * cube_pthread/lbm_ib.c:main) keeps its types and call sequence:
+ *
+ *     init_gv_constant(gv);                      mpi/init_gv.c:49
+ *     gen_fluid_grid(gv->fluid_grid, cs, 0, gv); mpi/gen_fluid_grid.c:25
+ *     gen_fiber_sheet(&gv->fiber_shape->sheets[k]);   mpi/gen_fiber_sheet.c:25
+ *     init_gv(gv);                               mpi/init_gv.c:117
+ *     init_eqlbrmdistrfuncDF0(gv); init_df1(gv); init_df_inout(gv);
+ *     do_thread(lv);                             mpi/do_thread.c:36
+ *
+ * and links liblbib.so instead of the reference's kernel objects.  The
+ * populations, forces and sheet state then live in GPU memory; the host-side
+ * Fibernode arrays are refreshed by lbib_sync_to_host() and by the dump
+ * writers.  Every function keeps the reference's argument meaning.  Where the
+ * reference printed and called exit(1) (a fiber stencil leaving the grid,
+ * cube_pthread/lbm_ib.c:1458-1466), this library records a sticky error code
+ * (lbib_last_error) and the step loop stops.
+ *
+ * Numerics: FP64 throughout, the same floating-point operations in the same
+ * order as the reference (no contraction), so that results match the
+ * reference bit for bit except through the cosine of the delta kernel, which
+ * is correctly rounded here (the host C library's cosine is not).
+ */
+#ifndef LBIB_H
+#define LBIB_H
+
+#include <pthread.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- data model: field names of mpi/do_thread.h:96-239 ------------------ */
+
+/* mpi/do_thread.h:96-101, cube_pthread/lbm_ib.c:54-59 */
+typedef struct fiber_node_t {
+  double x, y, z;
+  double bend_force_x, bend_force_y, bend_force_z;
+  double stretch_force_x, stretch_force_y, stretch_force_z;
+  double elastic_force_x, elastic_force_y, elastic_force_z;
+} Fibernode;
+
+/* mpi/do_thread.h:104-107 */
+typedef struct fiber_t {
+  Fibernode* nodes;
+  int num_nodes;
+} Fiber;
+
+/* mpi/do_thread.h:110-119: width along z, height along y */
+typedef struct fiber_sheet_t {
+  Fiber* fibers;
+  double width, height;
+  int num_cols, num_rows;
+  double x_orig, y_orig, z_orig;
+} Fibersheet;
+
+/* mpi/do_thread.h:122-125 */
+typedef struct fiber_shape_t {
+  Fibersheet* sheets;
+  int num_sheets;
+} Fibershape;
+
+/* mpi/do_thread.h:131-139: the reference's 824-byte AoS cell.  Only the
+ * dump writers materialise it (for the cells they write); the solver keeps
+ * structure-of-arrays populations in GPU memory. */
+typedef struct fluid_node_t {
+  double vel_x, vel_y, vel_z;
+  double rho, pressure;
+  double df1[19];
+  double df2[19];
+  double dfeq[19];
+  double df_inout[2][19];
+  double elastic_force_x, elastic_force_y, elastic_force_z;
+} Fluidnode;
+
+/* mpi/do_thread.h:142-145 */
+typedef struct fluid_surface_t {
+  Fluidnode* nodes;
+} Fluidsurface;
+
+/* mpi/do_thread.h:150-161 */
+typedef struct sub_fluid_grid_t {
+  int sub_coordx_start, sub_coordx_end;
+  int sub_coordy_start, sub_coordy_end;
+  int sub_coordz_start, sub_coordz_end;
+  Fluidnode* nodes;
+  bool isboundary;
+  int grid_dim_x;
+  int grid_dim_y;
+  int grid_dim_z;
+} Sub_Fluidgrid;
+
+/* mpi/do_thread.h:166-175.  x is the flow direction (inlet at x = 1, 2,
+ * outlet at x = x_dim-3, x_dim-2).  inlet/outlet/sub_fluid_grid stay NULL:
+ * the populations live on the GPU. */
+typedef struct fluid_grid_t {
+  int x_dim;
+  int y_dim;
+  int z_dim;
+  int num_cubes_x, num_cubes_y, num_cubes_z;
+  Fluidsurface* inlet;
+  Fluidsurface* outlet;
+  Sub_Fluidgrid* sub_fluid_grid;
+} Fluidgrid;
+
+struct lbib_device;  /* GPU-resident state, owned by this library */
+
+/* mpi/do_thread.h:178-239 minus the MPI message buffers, plus the pthread
+ * variant's TIME_STOP/c/P/Q/R/total_threads/num_cubes_* fields
+ * (cube_pthread/lbm_ib.c:126-159), plus three fields of this library. */
+typedef struct gv_t {
+  Fibershape* fiber_shape;
+  Fluidgrid* fluid_grid;
+  double tau, nu_l, u_l, rho_l, L_l, M_l, g_l, Ks_l, Kb_l, Kst_l;
+  double Re, cs_l, Ma, Kn, Kshat, Ksthat, Kbhat, Mhat, Fr;
+  int dt, time, timesteps, dump;
+  int TIME_STOP;                   /* pthread name of the last step      */
+  double c[19][3];                 /* lattice velocities (pthread GV)    */
+  int ib, ie, jb, je, kb, ke;
+  int tx, ty, tz;
+  int threads_per_task;
+  int P, Q, R, total_threads;
+  int num_cubes_x, num_cubes_y, num_cubes_z;
+  int cube_size;
+  pthread_t* threads;
+  pthread_mutex_t* lock_Fluid;
+  pthread_barrier_t barr;
+  int taskid;
+  int num_fluid_tasks;
+  /* ---- additions of this library ---- */
+  struct lbib_device* dev;         /* NULL until gen_fluid_grid          */
+  int lbib_compat;                 /* LBIB_COMPAT_* bits, see below      */
+  int lbib_dump_mode;              /* LBIB_DUMP_* bits for do_thread     */
+}* GV;
+
+/* mpi/do_thread.h:242-245 */
+typedef struct lv_t {
+  int tid;
+  GV gv;
+}* LV;
+
+/* Reference behaviours kept for parity; all are set by init_gv_constant.
+ * Clearing a bit selects the corrected behaviour. */
+#define LBIB_COMPAT_BEND_X_BUG    1  /* x[j] for x[j-2] at col = cols-2, cube_pthread/lbm_ib.c:1032-1035 */
+#define LBIB_COMPAT_YWALL_CUBES_X 2  /* y-wall z range clipped with num_cubes_x, lbm_ib.c:2378,2414 */
+#define LBIB_COMPAT_INOUT_PTHREAD 4  /* inlet/outlet copy loops BK < num_cubes_x, lbm_ib.c:2800-2882 */
+#define LBIB_COMPAT_ALL           7
+
+/* What do_thread writes at time == 1 and every gv->dump steps. */
+#define LBIB_DUMP_NONE      0
+#define LBIB_DUMP_FIELDVIEW 1  /* FV_* files, cube_pthread/lbm_ib.c:3100-3112, 3519-3538 */
+#define LBIB_DUMP_BINARY    2  /* Fiber%d_dump_step%d.bin, mpi/do_thread.c:335-352 */
+
+/* Error codes returned by the int entry points and by lbib_last_error. */
+#define LBIB_OK              0
+#define LBIB_E_ARG          -1   /* bad size, NULL pointer, indivisible grid */
+#define LBIB_E_CUDA         -2   /* a CUDA call failed                       */
+#define LBIB_E_STENCIL      -3   /* a fiber stencil left the fluid grid      */
+#define LBIB_E_STATE        -4   /* call out of order (no grid, no sheet)    */
+#define LBIB_E_NOMEM        -5   /* device or host allocation failed         */
+#define LBIB_E_CAPACITY     -6   /* more touched force tiles than allocated  */
+#define LBIB_E_IO           -7   /* a dump file could not be written         */
+
+/* ---- set-up: mpi/init_gv.c, mpi/gen_*.c, mpi/init_*.c ----------------- */
+
+/* mpi/init_gv.c:49-99: dt, time, cube counts, ib..ke and the reference's
+ * hard-coded physics (Re 150, u_l 0.001, L 20, tau from nu, Kb_l, Ks_l).
+ * Needs gv->fluid_grid->{x,y,z}_dim and gv->cube_size. */
+void init_gv_constant(GV gv);
+
+/* mpi/gen_fluid_grid.c:25-68: allocates the GPU state for the grid
+ * described by fluid_grid (rho = rho_l, u = (u_l, 0, 0) everywhere).
+ * taskid is accepted for signature compatibility; one GPU owns the grid. */
+void gen_fluid_grid(Fluidgrid* fluid_grid, int cube_size, int taskid, GV gv);
+
+/* mpi/gen_fiber_sheet.c:25-68: allocates sheet->fibers and places node
+ * (row, col) at (x_orig, y_orig + row*height/(rows-1), z_orig + col*width/(cols-1)). */
+void gen_fiber_sheet(Fibersheet* sheet);
+
+/* mpi/init_gv.c:117-275: shifts every sheet by u_l*dt in x and uploads the
+ * sheets to the GPU. */
+void init_gv(GV gv);
+
+/* mpi/init_eqlbrmdistrfuncDF0.c:41-120, mpi/init_df1.c:13-56,
+ * mpi/init_df_inout.c:14-81: equilibrium populations, interior df1, and the
+ * fixed inlet (x = ib) / outlet (x = x_dim-1) planes, all on the GPU. */
+void init_eqlbrmdistrfuncDF0(GV gv);
+void init_df1(GV gv);
+void init_df_inout(GV gv);
+
+/* ---- the step: mpi/do_thread.c:36-403, cube_pthread/lbm_ib.c:3087-3570 -- */
+
+/* Runs steps while gv->time <= gv->timesteps (or TIME_STOP when timesteps
+ * is 0), dumping per gv->lbib_dump_mode when time % dump == 0 (and at
+ * time == 1 for FieldView, as the pthread code does).  Only tid 0 works;
+ * other tids return at once, so a host that still spawns T threads stays
+ * correct.  Returns NULL; check lbib_last_error(). */
+void* do_thread(void* v);
+
+/* The stages of one step, callable one by one in do_thread order.  On the
+ * GPU the fluid part is one fused in-place kernel: compute_eqlbrmdistrfuncDF1
+ * launches it (collision, streaming, bounce-back, inlet/outlet and the
+ * df2->df1 copy together); stream_distrfunc, bounceback_rigidwalls and
+ * copy_inout_to_df2 are then no-ops, and replace_old_DF closes the step.
+ * Calling them out of order is undefined. */
+void compute_bendingforce(LV lv);        /* mpi/compute_bendingforce.c:25      */
+void compute_stretchingforce(LV lv);     /* mpi/compute_stretchingforce.c:25   */
+void compute_elasticforce(LV lv);        /* mpi/compute_elasticforce.c:25      */
+void fiber_SpreadForce(LV lv);           /* mpi/fiber_SpreadForce.c:64         */
+void fluid_get_SpreadForce(LV lv);       /* mpi/fluid_get_SpreadForce.c:28     */
+void get_influentialdomain_fluid_grid_and_SpreadForce(LV lv); /* lbm_ib.c:1323 */
+void compute_eqlbrmdistrfuncDF1(LV lv);  /* mpi/compute_eqlbrmdistrfuncDF1.c:75 */
+void stream_distrfunc(LV lv);            /* mpi/stream_distrfunc.c:232         */
+void bounceback_rigidwalls(LV lv);       /* mpi/bounceback_rigidwalls.c:25     */
+void compute_rho_and_u(LV lv);           /* mpi/compute_rho_and_u.c:27         */
+void fluid_SpreadVelocity(LV lv);        /* mpi/fluid_SpreadVelocity.c:25      */
+void fiber_get_SpreadVelocity(LV lv);    /* mpi/fiber_get_SpreadVelocity.c:47  */
+void moveFiberSheet(LV lv);              /* cube_pthread/lbm_ib.c:2540         */
+void copy_inout_to_df2(LV lv);           /* mpi/copy_inout_to_df2.c:13         */
+void replace_old_DF(LV lv);              /* mpi/replace_old_DF.c:13            */
+void periodicBC(LV lv);                  /* mpi/periodicBC.c:29, never called by
+                                            the reference loop; a no-op here   */
+
+/* ---- dumps: mpi/print_info.c, cube_pthread/lbm_ib.c:331-692 ------------ */
+void save_fiber_sub_grid(GV gv, int start_y, int start_z, int end_y, int end_z, char fName[]);
+void save_fiber_sub_grid_binary(GV gv, int start_y, int start_z, int end_y, int end_z, char fName[]);
+void save_fluid_sub_grid(GV gv, int start_x, int start_y, int start_z,
+                         int end_x, int end_y, int end_z, char fName[]);
+void save_fluid_sub_grid_vel_use_fv(GV gv, int start_x, int start_y, int start_z,
+                                    int end_x, int end_y, int end_z, char fName[]);
+void save_fluid_sub_grid_cord_use_fv(GV gv, int start_x, int start_y, int start_z,
+                                     int end_x, int end_y, int end_z, char fName[]);
+void save_fiber_sub_grid_cord_ef_use_fv(GV gv, int start_y, int start_z, int end_y, int end_z,
+                                        char grid_fname[], char elastic_force_fname[]);
+
+/* ---- additions (no reference counterpart) ----------------------------- */
+
+/* Overrides the physics that init_gv_constant hard-codes
+ * (mpi/init_gv.c:74-97).  Call before init_gv / init_eqlbrmdistrfuncDF0:
+ * it also resets the initial velocity to (u_l, 0, 0). */
+int lbib_set_params(GV gv, double tau, double u_l, double Ks_l, double Kb_l);
+int lbib_set_compat(GV gv, int flags);
+int lbib_last_error(void);
+const char* lbib_error_string(int code);
+void lbib_clear_error(void);
+/* Copies sheet positions and forces back into gv->fiber_shape. */
+int lbib_sync_to_host(GV gv);
+/* Frees everything this library allocated for gv (GPU state, sheets,
+ * fluid_grid planes); gv itself and the objects the caller made stay. */
+void lbib_free(GV gv);
+
+/* Array access for tests, tools and bindings (x-fastest scalar fields,
+ * idx = (z*y_dim + y)*x_dim + x; sheet records of 12 doubles in Fibernode
+ * order, row-major).  All return LBIB_OK or an error code. */
+int lbib_get_moments(GV gv, double* rho, double* ux, double* uy, double* uz);
+int lbib_get_force(GV gv, double* fx, double* fy, double* fz);
+int lbib_get_df1(GV gv, double* out);            /* [19][N], cells of [2,n-3]^3 */
+int lbib_get_sheet(GV gv, int sheet, double* out);
+int lbib_set_sheet(GV gv, int sheet, const double* in);
+int lbib_run(GV gv, int nsteps);                 /* do_thread for nsteps steps */
+int lbib_device_count(void);                     /* CUDA devices visible (0 if none) */
+int lbib_synchronize(GV gv);
+void* lbib_stream(GV gv);                        /* the cudaStream_t used */
+long lbib_kernel_launches(GV gv);                /* CUDA kernels launched so far */
+/* Stage timing with CUDA events on the library's stream: between begin and
+ * end every step records events around its five stages; end synchronises and
+ * returns the summed milliseconds of [fiber forces, spread, fused fluid step,
+ * tile moments, interpolate+move] and the number of steps timed. */
+int lbib_profile_begin(GV gv);
+int lbib_profile_end(GV gv, double* stage_ms, long* steps);
+
+/* One-call set-up used by bindings: the sequence init_gv_constant,
+ * gen_fluid_grid, gen_fiber_sheet (each sheet), init_gv, lbib_set_params,
+ * init_eqlbrmdistrfuncDF0, init_df1, init_df_inout.  Returns a GV owned by
+ * the library (free with lbib_case_free) or NULL (see lbib_last_error). */
+GV lbib_case_create(int nx, int ny, int nz, int cube_size, int nsheets,
+                    const int* rows, const int* cols,
+                    const double* width, const double* height,
+                    const double* x0, const double* y0, const double* z0,
+                    double tau, double u_l, double Ks_l, double Kb_l, int compat);
+void lbib_case_free(GV gv);
+/* Calls one stage by number, in do_thread order: 0 bending, 1 stretching,
+ * 2 elastic, 3 spread (fiber_SpreadForce + fluid_get_SpreadForce),
+ * 4 compute_eqlbrmdistrfuncDF1, 5 stream, 6 bounce-back, 7 rho and u,
+ * 8 interpolate and move, 9 inlet/outlet copy, 10 replace_old_DF. */
+int lbib_stage(GV gv, int which);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,168 @@
+"""CUDA path vs the oracle and vs the reference's own results.
+
+Two bars, both stated here:
+* against the oracle built with the same correctly rounded delta-kernel
+  cosine (liboracle_cr.so) the CUDA path must be bit-identical -- every
+  stage keeps the reference's FP64 operation order;
+* against the reference itself (fixtures from oracle/_ref, which uses the C
+  library's cosine, ~0.1% of whose values are 1 ulp off) the relative L2
+  error of rho, of u as a vector field and of the fiber positions must be
+  <= 1e-10.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import lbib
+import pyoracle as P
+from cases import SMALL_CASES, c0_case, small_case
+from pyoracle import Case, Sheet, centred_sheet
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-10
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def interior(case):
+    return (slice(2, case.nz - 2), slice(2, case.ny - 2), slice(2, case.nx - 2))
+
+
+def assert_same_state(s, o, case, check_df=True):
+    for name, a, b in zip(["rho", "ux", "uy", "uz"], s.moments(), o.moments()):
+        np.testing.assert_array_equal(a, b, err_msg=name)
+    for k in range(len(case.sheets)):
+        np.testing.assert_array_equal(s.sheet(k), o.sheet(k), err_msg=f"sheet {k}")
+    for name, a, b in zip(["fx", "fy", "fz"], s.force(), o.force()):
+        np.testing.assert_array_equal(a, b, err_msg=name)
+    if check_df:
+        g = s.df1()[(slice(None),) + interior(case)]
+        r = o.df(0)[(slice(None),) + interior(case)]
+        np.testing.assert_array_equal(g, r, err_msg="df1")
+
+
+EXTRA_CASES = {
+    "no_compat_xltz": (small_case(12, 12, 24, 6, 6, 5.0, compat=0), 20),
+    "bend_fixed": (small_case(24, 12, 12, 6, 6, 8.0, compat=P.COMPAT_ALL & ~P.COMPAT_BEND_X_BUG), 20),
+    "passive": (small_case(24, 12, 12, 6, 6, 8.0, Ks_l=0.0, Kb_l=0.0), 20),
+    "two_sheets": (Case(40, 16, 16, [centred_sheet(40, 16, 16, 6, 6, 0.5, 9.0),
+                                     centred_sheet(40, 16, 16, 8, 4, 0.5, 24.0)]), 15),
+    "cube8": (small_case(32, 16, 24, 8, 8, 10.0, cube_size=8), 15),
+    "xeqz": (small_case(16, 12, 16, 6, 6, 6.0), 15),
+}
+
+
+@pytest.mark.parametrize("name", list(SMALL_CASES) + list(EXTRA_CASES))
+def test_bitexact_vs_oracle_cr(gpu, oracle_built, name):
+    case, steps = {**SMALL_CASES, **EXTRA_CASES}[name]
+    s = lbib.Solver(case)
+    o = P.Oracle(case, cr_cos=True)
+    assert_same_state(s, o, case)          # initial state
+    s.run(1); o.run(1)
+    assert_same_state(s, o, case)          # first step (initial moments, no zero links)
+    s.run(steps - 1); o.run(steps - 1)
+    assert_same_state(s, o, case)
+    s.close()
+
+
+@pytest.mark.parametrize("name", list(SMALL_CASES))
+def test_vs_reference_golden(gpu, name):
+    case, steps = SMALL_CASES[name]
+    g = np.load(os.path.join(GOLDEN, f"small_{name}.npz"))
+    s = lbib.Solver(case)
+    s.run(int(g["steps"]))
+    rho, ux, uy, uz = s.moments()
+    assert rel_l2(rho, g["rho"]) <= TOL
+    assert rel_l2(np.stack([ux, uy, uz]), np.stack([g["ux"], g["uy"], g["uz"]])) <= TOL
+    assert rel_l2(s.sheet()[..., :3], g["sheet"][..., :3]) <= TOL
+    # at these lengths the cosine's last bit has not grown: also per component
+    for a, b in [(ux, g["ux"]), (uy, g["uy"]), (uz, g["uz"])]:
+        assert np.max(np.abs(a - b)) <= TOL * np.max(np.abs(b))
+    s.close()
+
+
+def test_stagewise_vs_oracle_cr(gpu, oracle_built):
+    """Each IB stage alone on a deformed sheet, after a few full steps."""
+    case, _ = SMALL_CASES["wall"]
+    s = lbib.Solver(case)
+    o = P.Oracle(case, cr_cos=True)
+    s.run(5); o.run(5)
+    rng = np.random.default_rng(7)
+    sh = o.sheet().copy()
+    sh[..., :3] += rng.uniform(-0.3, 0.3, size=sh[..., :3].shape)
+    s.set_sheet(0, sh); o.set_sheet(0, sh)
+    s.stage("bending"); s.stage("stretching"); s.stage("elastic")
+    o.stage("bending"); o.stage("stretching"); o.stage("elastic")
+    np.testing.assert_array_equal(s.sheet(), o.sheet())
+    s.stage("spread"); assert o.stage("spread") == 0
+    for a, b in zip(s.force(), o.force()):
+        np.testing.assert_array_equal(a, b)
+    for st in ["collide", "stream", "bounceback", "moments", "move", "copy_inout", "replace"]:
+        s.stage(st)
+    for st in ["collide", "stream", "bounceback", "moments", "move", "copy_inout", "replace"]:
+        o.stage(st)
+    np.testing.assert_array_equal(s.sheet(), o.sheet())
+    for a, b in zip(s.moments(), o.moments()):
+        np.testing.assert_array_equal(a, b)
+    s.close()
+
+
+def test_deterministic(gpu):
+    case, steps = SMALL_CASES["base"]
+    a = lbib.Solver(case); b = lbib.Solver(case)
+    a.run(steps); b.run(steps)
+    for x, y in zip(a.moments() + [a.sheet()], b.moments() + [b.sheet()]):
+        assert x.tobytes() == y.tobytes()
+    a.close(); b.close()
+
+
+def test_stencil_leaving_grid_is_an_error(gpu):
+    """The reference exits when a stencil leaves the grid
+    (cube_pthread/lbm_ib.c:1458-1466); here the step loop stops with an error."""
+    nx, ny, nz = 24, 12, 12
+    case = Case(nx, ny, nz, [Sheet(6, 6, 2.5, 2.5, 3.2, 4.0, 4.0)], u_l=0.05)
+    s = lbib.Solver(case)
+    sh = s.sheet().copy()
+    sh[..., 0] = 0.5          # stencil start floor(0.5 - 2) + 1 = -1
+    s.set_sheet(0, sh)
+    with pytest.raises(lbib.LbibError, match="stencil"):
+        s.run(3)
+    s.close()
+
+
+@pytest.mark.slow
+def test_c0_1000_steps(gpu):
+    """The reference's own workload (128x64x64, 52x52 sheet) for 1000 steps:
+    bit-identical to the oracle with the correctly rounded cosine, and within
+    1e-10 relative L2 of the reference itself."""
+    case = c0_case()
+    s = lbib.Solver(case)
+    s.run(1000)
+    rho, ux, uy, uz = s.moments()
+    sheet = s.sheet()
+    ref = json.load(open(os.path.join(GOLDEN, "c0_1000_cr.json")))
+    import hashlib
+
+    def h(fields):
+        m = hashlib.sha256()
+        for a in fields:
+            m.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+        return m.hexdigest()
+    assert h([rho, ux, uy, uz]) == ref["moments_sha256"]
+    assert h([sheet]) == ref["sheet_sha256"]
+    g = np.load(os.path.join(GOLDEN, "c0_1000.npz"))
+    idx = g["sample_idx"]
+    assert rel_l2(sheet[..., :3], g["sheet"][..., :3]) <= TOL
+    assert rel_l2(rho.ravel()[idx], g["rho"]) <= TOL
+    u = np.stack([ux.ravel()[idx], uy.ravel()[idx], uz.ravel()[idx]])
+    assert rel_l2(u, np.stack([g["ux"], g["uy"], g["uz"]])) <= TOL
+    norms = np.array([np.linalg.norm(rho), np.linalg.norm(ux), np.linalg.norm(uy), np.linalg.norm(uz)])
+    np.testing.assert_allclose(norms, g["norms"], rtol=TOL)
+    s.close()
