@@ -72,6 +72,8 @@ CONFIGS = {
     "c1": dict(nx=512, ny=256, nz=256, rows=208, cols=208, x0=80.0),
     # the reference's own size: 128 x 64 x 64, 52 x 52 sheet at x = 20
     "c0": dict(nx=128, ny=64, nz=64, rows=52, cols=52, x0=20.0),
+    # c1 at half size per axis (populations 637 MB, above L2): for ncu captures
+    "p1": dict(nx=256, ny=128, nz=128, rows=104, cols=104, x0=40.0),
 }
 
 
@@ -175,9 +177,10 @@ def dist_env():
 
 
 class Group:
-    """torch.distributed over NCCL for the barrier and the max over ranks."""
+    """torch.distributed for the barrier and the max over ranks: NCCL, one
+    rank per GPU, on a GPU box; gloo when there is no GPU (host-side tests)."""
 
-    def __init__(self, world, local):
+    def __init__(self, world, local, backend=None, timeout_s=300):
         self.world = world
         self.dist = None
         if world > 1:
@@ -185,9 +188,12 @@ class Group:
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", local))
+            self.backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+            kw = {}
+            if self.backend == "nccl":
+                torch.cuda.set_device(local)
+                kw["device_id"] = torch.device("cuda", local)
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
             self.dist = dist
             self.torch = torch
 
@@ -198,13 +204,19 @@ class Group:
     def max(self, v):
         if not self.dist:
             return v
-        t = self.torch.tensor([v], dtype=self.torch.float64, device="cuda")
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([v], dtype=self.torch.float64, device=dev)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.dist:
             self.dist.destroy_process_group()
+
+
+def whole_job_mlups(cells_per_rank, steps, world, max_seconds):
+    """Lattice updates of all replicas over the slowest rank's time."""
+    return cells_per_rank * steps * world / max_seconds / 1e6
 
 
 # ---------------------------------------------------------------- CPU legs
@@ -314,7 +326,7 @@ def run_lbib(args):
     ms = e0.elapsed_time(e1)
     group.barrier()
     ms_max = group.max(ms)
-    value = case.ncells * args.steps * world / (ms_max / 1e3) / 1e6
+    value = whole_job_mlups(case.ncells, args.steps, world, ms_max / 1e3)
 
     fluid_cells = (case.nx - 4) * (case.ny - 4) * (case.nz - 4)
     bytes_launch = fluid_cells * BYTES_PER_UPDATE
@@ -342,7 +354,7 @@ def run_lbib(args):
         e2e_s = group.max(t1 - t0)
         h2d = S * 96
         d2h = S * 96 + 4 * 8 * case.ncells / args.steps
-        e2e = {"value": case.ncells * args.steps * world / e2e_s / 1e6, "unit": UNIT,
+        e2e = {"value": whole_job_mlups(case.ncells, args.steps, world, e2e_s), "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h,
                "how": "lbib_set_sheet + init_df1/init_df_inout, then per step do_thread(1 step) + "
                       "lbib_sync_to_host, then lbib_get_moments; wall clock, max over ranks"}

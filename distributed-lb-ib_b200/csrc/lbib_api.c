@@ -387,11 +387,8 @@ int lbib_sync_to_host(GV gv) {
   if (!gv || !gv->dev || !gv->fiber_shape) return set_error(LBIB_E_STATE);
   long S = total_nodes(gv);
   if (S != gv->dev->S) return set_error(LBIB_E_STATE);
-  double* buf = (double*)malloc(sizeof(double) * 12 * S);
-  if (!buf) return set_error(LBIB_E_NOMEM);
-  int rc = lbdev_get_nodes(gv->dev, buf);
-  if (!rc) unpack_nodes(gv, buf);
-  free(buf);
+  int rc = lbdev_get_nodes(gv->dev, NULL);  /* into the pinned staging buffer */
+  if (!rc) unpack_nodes(gv, gv->dev->h_nodes);
   return rc ? set_error(rc) : LBIB_OK;
 }
 

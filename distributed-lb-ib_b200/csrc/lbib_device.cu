@@ -37,12 +37,18 @@ static void free_tiles(lbib_device* d) {
     cudaFree(d->Ftile[b]); d->Ftile[b] = NULL;
     cudaFree(d->Utile[b]); d->Utile[b] = NULL;
   }
-  cudaFree(d->tile_flag); d->tile_flag = NULL;
+  cudaFree(d->tile_cnt); d->tile_cnt = NULL;
+  cudaFree(d->slot_off); d->slot_off = NULL;
+  cudaFree(d->slot_len); d->slot_len = NULL;
+  cudaFree(d->slot_cursor); d->slot_cursor = NULL;
+  cudaFree(d->pair_node); d->pair_node = NULL;
   cudaFree(d->scan_tmp); d->scan_tmp = NULL;
 }
 
 static void free_sheets(lbib_device* d) {
   cudaFree(d->nodes); d->nodes = NULL;
+  if (d->h_nodes) cudaFreeHost(d->h_nodes);
+  d->h_nodes = NULL;
   cudaFree(d->W); d->W = NULL;
   cudaFree(d->st); d->st = NULL;
   cudaFree(d->chunk_box); d->chunk_box = NULL;
@@ -81,12 +87,43 @@ static void derive_boundaries(lbib_device* d) {
   if ((d->compat & 2) && d->ncx < d->ncz) d->yskip_z0 = d->ncx * d->cube_size - 2;
 }
 
+extern "C" int lbdev_bulk_rows(const lbib_device* d, int* nrows_y, int* nrows_z);
+
+/* Rows (y, z) of I that the generic fused kernel processes: all of them, or,
+ * with the staged kernel on, those it does not take (next to the walls, or
+ * above zin_hi).  The staged kernel needs even nx for aligned copies. */
+static int build_rows(lbib_device* d) {
+  const char* env = getenv("LBIB_FLUID_BULK");
+  int ry = 0, rz = 0;
+  d->use_bulk = !(env && env[0] == '0') && (d->nx % 2 == 0) && lbdev_bulk_rows(d, &ry, &rz);
+  const int zb = 2 + rz;  /* last z row of the staged kernel */
+  long cap = (long)(d->ny - 4) * (d->nz - 4);
+  int* h = (int*)malloc(sizeof(int) * 2 * cap);
+  if (!h) return -5;
+  int n = 0;
+  for (int z = 2; z <= d->nz - 3; ++z)
+    for (int y = 2; y <= d->ny - 3; ++y) {
+      const int bulk = d->use_bulk && y >= 3 && y <= d->ny - 4 && z >= 3 && z <= zb;
+      if (!bulk) { h[2 * n] = y; h[2 * n + 1] = z; ++n; }
+    }
+  cudaFree(d->rows);
+  d->rows = NULL;
+  d->nrows = n;
+  int rc = 0;
+  if (n > 0) {
+    if (cudaMalloc(&d->rows, sizeof(int) * 2 * n) != cudaSuccess) rc = -5;
+    else if (cudaMemcpy(d->rows, h, sizeof(int) * 2 * n, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
+  }
+  free(h);
+  return rc;
+}
+
 extern "C" int lbdev_set_physics(lbib_device* d, const lbdev_config* c) {
   d->tau = c->tau; d->u_l = c->u_l; d->rho_l = c->rho_l; d->Ks_l = c->Ks_l; d->Kb_l = c->Kb_l;
   d->g_l = c->g_l; d->cs_l = c->cs_l; d->dt = c->dt; d->compat = c->compat;
   derive_constants(d);
   derive_boundaries(d);
-  return 0;
+  return d->stream ? build_rows(d) : 0;
 }
 
 extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
@@ -113,6 +150,7 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   if (!rc && cudaMallocHost(&d->h_err, sizeof(int) * 2) != cudaSuccess) rc = -5;
   if (!rc && cudaMemsetAsync(d->err, 0, sizeof(int) * 2, d->stream) != cudaSuccess) rc = -2;
   if (!rc && cudaMemsetAsync(d->f, 0, sizeof(double) * 19 * d->N, d->stream) != cudaSuccess) rc = -2;
+  if (!rc) rc = build_rows(d);
   if (rc) { lbdev_free(d); return rc; }
   d->cur = 0;
   *out = d;
@@ -124,7 +162,7 @@ extern "C" void lbdev_free(lbib_device* d) {
   if (d->stream) cudaStreamSynchronize(d->stream);
   free_tiles(d);
   free_sheets(d);
-  cudaFree(d->f); cudaFree(d->inlet); cudaFree(d->outlet); cudaFree(d->err);
+  cudaFree(d->f); cudaFree(d->inlet); cudaFree(d->outlet); cudaFree(d->err); cudaFree(d->rows);
   cudaFree(d->scratch);
   for (long i = 0; i < 6 * d->prof_cap; ++i) cudaEventDestroy(d->prof_ev[i]);
   free(d->prof_ev);
@@ -146,6 +184,7 @@ extern "C" int lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_de
     free_tiles(d);
     d->nchunks = (S + 31) / 32;
     CK(cudaMalloc(&d->nodes, sizeof(double) * 12 * S));
+    CK(cudaMallocHost(&d->h_nodes, sizeof(double) * 12 * S));
     CK(cudaMalloc(&d->W, sizeof(double) * 12 * S));
     CK(cudaMalloc(&d->st, sizeof(int) * 3 * S));
     CK(cudaMalloc(&d->chunk_box, sizeof(int) * 6 * d->nchunks));
@@ -160,8 +199,12 @@ extern "C" int lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_de
       CK(cudaMemsetAsync(d->tile_slot[b], 0xff, sizeof(int) * d->ntiles, d->stream));
       CK(cudaMemsetAsync(d->tile_count[b], 0, sizeof(int), d->stream));
     }
-    CK(cudaMalloc(&d->tile_flag, sizeof(int) * d->ntiles));
-    CK(cudaMalloc(&d->scan_tmp, sizeof(int) * ((d->ntiles + 1023) / 1024 + 1)));
+    CK(cudaMalloc(&d->tile_cnt, sizeof(int) * d->ntiles));
+    CK(cudaMalloc(&d->slot_off, sizeof(int) * d->cap));
+    CK(cudaMalloc(&d->slot_len, sizeof(int) * d->cap));
+    CK(cudaMalloc(&d->slot_cursor, sizeof(int) * d->cap));
+    CK(cudaMalloc(&d->pair_node, sizeof(int) * 8 * S));
+    CK(cudaMalloc(&d->scan_tmp, sizeof(int) * 2 * ((d->ntiles + 1023) / 1024 + 1)));
   }
   free(d->sh);
   d->sh = (lbib_sheet_dev*)malloc(sizeof(lbib_sheet_dev) * nsheets);
@@ -362,9 +405,12 @@ extern "C" int lbdev_get_df1(lbib_device* d, double* out) {
   return 0;
 }
 
+/* Sheet records to host memory; out == NULL leaves them in the pinned
+ * staging buffer d->h_nodes. */
 extern "C" int lbdev_get_nodes(lbib_device* d, double* out) {
-  CK(cudaMemcpyAsync(out, d->nodes, sizeof(double) * 12 * d->S, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaMemcpyAsync(d->h_nodes, d->nodes, sizeof(double) * 12 * d->S, cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));
+  if (out) memcpy(out, d->h_nodes, sizeof(double) * 12 * d->S);
   return 0;
 }
 

@@ -19,11 +19,17 @@ using namespace lbib;
 
 namespace {
 
+/* Resident blocks per SM the register budget is sized for (128 threads each). */
+#ifndef LBIB_FLUID_MINB
+#define LBIB_FLUID_MINB 4
+#endif
+
 template <int PAR>
-__global__ void __launch_bounds__(128) lbib_fluid_step(FluidParams p) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  const int y = blockIdx.y + 2;
-  const int z = blockIdx.z + 2;
+__global__ void __launch_bounds__(128, LBIB_FLUID_MINB) lbib_fluid_step(FluidParams p, const int2* __restrict__ rows) {
+  const int x = blockIdx.y * blockDim.x + threadIdx.x + 2;
+  const int2 r = rows[blockIdx.x];
+  const int y = r.x;
+  const int z = r.y;
   if (x > p.nx - 3) return;
   const long idx = ((long)z * p.ny + y) * p.nx + x;
   const int kind = classify(p, x, y, z);
@@ -158,13 +164,20 @@ FluidParams make_params(lbib_device* d, int first) {
 
 }  // namespace
 
+extern "C" int lbdev_launch_fluid_bulk(lbib_device* d, const void* fluid_params);
+
+/* One fused step: the generic kernel over d->rows (all rows of I, or only
+ * the rows next to the walls when the staged kernel takes the others). */
 extern "C" int lbdev_launch_fluid_step(lbib_device* d) {
   FluidParams p = make_params(d, d->steps == 0);
-  dim3 block(128);
-  dim3 grid((unsigned)((d->nx - 4 + 127) / 128), (unsigned)(d->ny - 4), (unsigned)(d->nz - 4));
-  if (d->parity == 0) lbib_fluid_step<0><<<grid, block, 0, d->stream>>>(p);
-  else lbib_fluid_step<1><<<grid, block, 0, d->stream>>>(p);
-  d->kernel_launches++;
+  if (d->nrows > 0) {
+    dim3 block(128);
+    dim3 grid((unsigned)d->nrows, (unsigned)((d->nx - 4 + 127) / 128));
+    if (d->parity == 0) lbib_fluid_step<0><<<grid, block, 0, d->stream>>>(p, (const int2*)d->rows);
+    else lbib_fluid_step<1><<<grid, block, 0, d->stream>>>(p, (const int2*)d->rows);
+    d->kernel_launches++;
+  }
+  if (d->use_bulk && lbdev_launch_fluid_bulk(d, &p)) return -2;
   d->parity ^= 1;
   d->steps++;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;

@@ -10,14 +10,16 @@
  *                       the spread and the interpolation of the step), the 4^3
  *                       tiles the stencil touches, and per 32-node chunk the
  *                       bounding box of its stencils.
- *   lbib_compact_*      touched tiles -> dense list in tile order and
- *                       tile -> slot map (deterministic prefix sums).
+ *   lbib_compact_*      touched tiles -> dense list in tile order, tile -> slot
+ *                       map, and each slot's node-list offset (deterministic
+ *                       prefix sums); lbib_pair_scatter fills the lists.
  *   lbib_spread_gather  fiber_SpreadForce + fluid_get_SpreadForce
  *                       (lbm_ib.c:1323-1525) as a gather: one CTA per touched
- *                       tile, one thread per cell, nodes visited chunk by chunk
- *                       in global (sheet, row, col) order, so each cell sums
- *                       its contributions in exactly the reference's order --
- *                       deterministic, no atomics.
+ *                       tile sorts the tile's node list by node index in
+ *                       shared memory, then each thread (cell) sums the
+ *                       contributions in that order -- the reference's
+ *                       (sheet, row, col) order -- so the result is
+ *                       deterministic and needs no atomics on forces.
  *   lbib_move_nodes     moveFiberSheet (lbm_ib.c:2540-2723): one thread per
  *                       node sums u * w over its 64 stencil cells in the
  *                       reference's (x, y, z) order, then X += dt U.
@@ -138,8 +140,11 @@ __global__ void lbib_fiber_forces(double* __restrict__ nodes, int R, int C, doub
 
 __device__ __forceinline__ int stencil_start(double p) { return (int)(floor(p / 1.0 - 2) + 1); }
 
+/* Per node: stencil start, the twelve delta-kernel factors, a count for
+ * every 4^3 tile the stencil touches, and per 32-node chunk the bounding box
+ * of the chunk's stencils (used only for crowded tiles). */
 __global__ void lbib_node_prep(const double* __restrict__ nodes, long S, int nx, int ny, int nz, int ntx, int nty,
-                               double* __restrict__ W, int* __restrict__ st, int* __restrict__ tile_flag,
+                               double* __restrict__ W, int* __restrict__ st, int* __restrict__ tile_cnt,
                                int* __restrict__ chunk_box, int* err, int step) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -160,7 +165,7 @@ __global__ void lbib_node_prep(const double* __restrict__ nodes, long S, int nx,
     } else {
       for (int tz = ks >> 2; tz <= (ks + 3) >> 2; ++tz)
         for (int ty = js >> 2; ty <= (js + 3) >> 2; ++ty)
-          for (int tx = is >> 2; tx <= (is + 3) >> 2; ++tx) tile_flag[((long)tz * nty + ty) * ntx + tx] = 1;
+          for (int tx = is >> 2; tx <= (is + 3) >> 2; ++tx) atomicAdd(&tile_cnt[((long)tz * nty + ty) * ntx + tx], 1);
       b0 = is; b1 = is + 3; b2 = js; b3 = js + 3; b4 = ks; b5 = ks + 3;
     }
   }
@@ -179,30 +184,39 @@ __global__ void lbib_node_prep(const double* __restrict__ nodes, long S, int nx,
   }
 }
 
-/* Deterministic compaction of tile_flag: per-block counts, one-block scan,
- * then each block writes its touched tiles in index order. */
+/* Deterministic compaction of the tile counts, in tile-index order:
+ * per-block sums (touched tiles, node-tile pairs), a one-block scan of both,
+ * then every touched tile gets its slot and the offset of its node list. */
 constexpr int kScanBlock = 1024;
 
-__global__ void lbib_compact_count(const int* __restrict__ flag, long n, int* __restrict__ block_sum) {
-  __shared__ int s[32];
+__global__ void lbib_compact_count(const int* __restrict__ cnt, long n, int* __restrict__ block_tiles,
+                                   int* __restrict__ block_pairs) {
+  __shared__ int s[2][32];
   const long i = (long)blockIdx.x * kScanBlock + threadIdx.x;
-  int v = (i < n) ? (flag[i] != 0) : 0;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+  const int c = (i < n) ? cnt[i] : 0;
+  int v = c > 0, w = c;
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+    w += __shfl_xor_sync(0xffffffffu, w, o);
+  }
+  if ((threadIdx.x & 31) == 0) { s[0][threadIdx.x >> 5] = v; s[1][threadIdx.x >> 5] = w; }
   __syncthreads();
   if (threadIdx.x < 32) {
-    int w = s[threadIdx.x];
-    for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-    if (threadIdx.x == 0) block_sum[blockIdx.x] = w;
+    int a = s[0][threadIdx.x], b = s[1][threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (threadIdx.x == 0) { block_tiles[blockIdx.x] = a; block_pairs[blockIdx.x] = b; }
   }
 }
 
-__global__ void lbib_compact_scan(int* __restrict__ block_sum, int nblocks, int* __restrict__ total) {
+__device__ void block_exclusive_scan(int* __restrict__ a, int n, int* total) {
   __shared__ int s[kScanBlock];
   int carry = 0;
-  for (int base = 0; base < nblocks; base += kScanBlock) {
+  for (int base = 0; base < n; base += kScanBlock) {
     const int i = base + threadIdx.x;
-    const int v = (i < nblocks) ? block_sum[i] : 0;
+    const int v = (i < n) ? a[i] : 0;
     s[threadIdx.x] = v;
     __syncthreads();
     for (int o = 1; o < kScanBlock; o <<= 1) {
@@ -211,46 +225,157 @@ __global__ void lbib_compact_scan(int* __restrict__ block_sum, int nblocks, int*
       s[threadIdx.x] += t;
       __syncthreads();
     }
-    if (i < nblocks) block_sum[i] = carry + s[threadIdx.x] - v;
+    if (i < n) a[i] = carry + s[threadIdx.x] - v;
     const int last = s[kScanBlock - 1];
     __syncthreads();
     carry += last;
   }
-  if (threadIdx.x == 0) *total = carry;
+  if (threadIdx.x == 0 && total) *total = carry;
 }
 
-__global__ void lbib_compact_write(const int* __restrict__ flag, long n, const int* __restrict__ block_off,
-                                   int* __restrict__ list, int* __restrict__ slot) {
-  __shared__ int s[32];
+__global__ void lbib_compact_scan(int* __restrict__ block_tiles, int* __restrict__ block_pairs, int nblocks,
+                                  int* __restrict__ total_tiles) {
+  block_exclusive_scan(block_tiles, nblocks, total_tiles);
+  __syncthreads();
+  block_exclusive_scan(block_pairs, nblocks, nullptr);
+}
+
+__global__ void lbib_compact_write(const int* __restrict__ cnt, long n, const int* __restrict__ block_tiles,
+                                   const int* __restrict__ block_pairs, int* __restrict__ list,
+                                   int* __restrict__ slot, int* __restrict__ slot_off, int* __restrict__ slot_len,
+                                   int* __restrict__ slot_cursor) {
+  __shared__ int sv[32], sw[32];
   const long i = (long)blockIdx.x * kScanBlock + threadIdx.x;
-  const int v = (i < n) ? (flag[i] != 0) : 0;
-  const unsigned bal = __ballot_sync(0xffffffffu, v);
+  const int c = (i < n) ? cnt[i] : 0;
+  const int v = c > 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) s[warp] = __popc(bal);
+  int iv = v, iw = c;  /* inclusive warp scans */
+  for (int o = 1; o < 32; o <<= 1) {
+    const int tv = __shfl_up_sync(0xffffffffu, iv, o);
+    const int tw = __shfl_up_sync(0xffffffffu, iw, o);
+    if (lane >= o) { iv += tv; iw += tw; }
+  }
+  if (lane == 31) { sv[warp] = iv; sw[warp] = iw; }
   __syncthreads();
   if (threadIdx.x < 32) {
-    int w = s[threadIdx.x];
-    int incl = w;
+    const int a = sv[threadIdx.x], b = sw[threadIdx.x];
+    int ia = a, ib = b;
     for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
+      const int ta = __shfl_up_sync(0xffffffffu, ia, o);
+      const int tb = __shfl_up_sync(0xffffffffu, ib, o);
+      if (lane >= o) { ia += ta; ib += tb; }
     }
-    s[threadIdx.x] = incl - w;
+    sv[threadIdx.x] = ia - a;
+    sw[threadIdx.x] = ib - b;
   }
   __syncthreads();
   if (v) {
-    const int pos = block_off[blockIdx.x] + s[warp] + __popc(bal & ((1u << lane) - 1u));
+    const int pos = block_tiles[blockIdx.x] + sv[warp] + iv - v;
     list[pos] = (int)i;
     slot[i] = pos;
+    slot_off[pos] = block_pairs[blockIdx.x] + sw[warp] + iw - c;
+    slot_len[pos] = c;
+    slot_cursor[pos] = 0;
   }
 }
 
-/* One CTA (64 threads = one 4^3 tile) per touched tile. */
+/* Every node appends its index to the list of each tile its stencil touches
+ * (order within a list is fixed afterwards by sorting). */
+__global__ void lbib_pair_scatter(const int* __restrict__ st, long S, int ntx, int nty, int nx, int ny, int nz,
+                                  const int* __restrict__ slot, const int* __restrict__ slot_off,
+                                  int* __restrict__ slot_cursor, int* __restrict__ pair_node,
+                                  const int* err) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S || *(volatile const int*)err) return;
+  const int is = st[i * 3 + 0], js = st[i * 3 + 1], ks = st[i * 3 + 2];
+  if (is < 0 || is + 3 >= nx || js < 0 || js + 3 >= ny || ks < 0 || ks + 3 >= nz) return;
+  for (int tz = ks >> 2; tz <= (ks + 3) >> 2; ++tz)
+    for (int ty = js >> 2; ty <= (js + 3) >> 2; ++ty)
+      for (int tx = is >> 2; tx <= (is + 3) >> 2; ++tx) {
+        const int s = slot[((long)tz * nty + ty) * ntx + tx];
+        const int k = atomicAdd(&slot_cursor[s], 1);
+        pair_node[slot_off[s] + k] = (int)i;
+      }
+}
+
+/* Longest per-tile node list sorted in shared memory; longer lists take the
+ * chunk-scan path below. */
+constexpr int kListCap = 1024;
+
+/* One CTA (64 threads = one 4^3 tile) per touched tile: sort the tile's node
+ * list by node index, then every cell adds the contributions of the nodes
+ * whose stencil contains it in that order -- the reference's order. */
 __global__ void __launch_bounds__(64) lbib_spread_gather(const double* __restrict__ nodes, const double* __restrict__ W,
-                                                         const int* __restrict__ st, const int* __restrict__ chunk_box,
-                                                         long S, long nchunks, const int* __restrict__ list,
-                                                         const int* __restrict__ count, int ntx, int nty,
-                                                         double* __restrict__ Ftile, const int* err) {
+                                                         const int* __restrict__ st, const int* __restrict__ list,
+                                                         const int* __restrict__ count, const int* __restrict__ slot_off,
+                                                         const int* __restrict__ slot_len, const int* __restrict__ pair_node,
+                                                         int ntx, int nty, double* __restrict__ Ftile, const int* err) {
+  __shared__ int ids[kListCap];
+  __shared__ int s_st[64][3];
+  __shared__ double s_w[64][12];
+  __shared__ double s_fe[64][3];
+  if (*(volatile const int*)err) return;
+  const int n = *count;
+  const int t = threadIdx.x;
+  const double cf = 1.0 / (64.0 * 1.0 * 1.0 * 1.0);
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const int L = slot_len[it];
+    if (L > kListCap) continue;
+    int P = 1;
+    while (P < L) P <<= 1;
+    const int* src = pair_node + slot_off[it];
+    __syncthreads();
+    for (int k = t; k < P; k += 64) ids[k] = (k < L) ? src[k] : INT_MAX;
+    __syncthreads();
+    for (int k = 2; k <= P; k <<= 1)
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int a = t; a < P; a += 64) {
+          const int b = a ^ j;
+          if (b > a) {
+            const int va = ids[a], vb = ids[b];
+            const bool up = (a & k) == 0;
+            if ((va > vb) == up) { ids[a] = vb; ids[b] = va; }
+          }
+        }
+        __syncthreads();
+      }
+    const int tile = list[it];
+    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+    const int gx = tx * 4 + (t & 3), gy = ty * 4 + ((t >> 2) & 3), gz = tz * 4 + (t >> 4);
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    for (int b0 = 0; b0 < L; b0 += 64) {
+      const int nb = min(64, L - b0);
+      if (t < nb) {
+        const long nd = ids[b0 + t];
+        s_st[t][0] = st[nd * 3 + 0]; s_st[t][1] = st[nd * 3 + 1]; s_st[t][2] = st[nd * 3 + 2];
+        for (int a = 0; a < 12; ++a) s_w[t][a] = W[nd * 12 + a];
+        s_fe[t][0] = nodes[nd * 12 + 9]; s_fe[t][1] = nodes[nd * 12 + 10]; s_fe[t][2] = nodes[nd * 12 + 11];
+      }
+      __syncthreads();
+      for (int j = 0; j < nb; ++j) {
+        const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
+        if ((unsigned)a < 4u && (unsigned)b < 4u && (unsigned)e < 4u) {
+          const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
+          Fx = Fx + s_fe[j][0] * tmp;
+          Fy = Fy + s_fe[j][1] * tmp;
+          Fz = Fz + s_fe[j][2] * tmp;
+        }
+      }
+      __syncthreads();
+    }
+    double* Ft = Ftile + (long)it * 192;
+    Ft[t] = Fx; Ft[64 + t] = Fy; Ft[128 + t] = Fz;
+  }
+}
+
+/* Crowded tiles (more than kListCap nodes, e.g. a crumpled sheet): visit the
+ * nodes chunk by chunk in global order, skipping chunks whose stencil box
+ * misses the tile.  Same summation order, no list needed. */
+__global__ void __launch_bounds__(64) lbib_spread_gather_scan(const double* __restrict__ nodes, const double* __restrict__ W,
+                                                              const int* __restrict__ st, const int* __restrict__ chunk_box,
+                                                              long S, long nchunks, const int* __restrict__ list,
+                                                              const int* __restrict__ count, const int* __restrict__ slot_len,
+                                                              int ntx, int nty, double* __restrict__ Ftile, const int* err) {
   __shared__ int hit[64];
   __shared__ int s_st[32][3];
   __shared__ double s_w[32][12];
@@ -260,6 +385,7 @@ __global__ void __launch_bounds__(64) lbib_spread_gather(const double* __restric
   const int cell = threadIdx.x;
   const double cf = 1.0 / (64.0 * 1.0 * 1.0 * 1.0);
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    if (slot_len[it] <= kListCap) continue;
     const int tile = list[it];
     const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
     const int x0 = tx * 4, y0 = ty * 4, z0 = tz * 4;
@@ -371,20 +497,27 @@ extern "C" int lbdev_launch_fiber_forces(lbib_device* d, int k) {
 extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
   const int c = d->cur;
   cudaStream_t st = d->stream;
-  if (cudaMemsetAsync(d->tile_flag, 0, d->ntiles * sizeof(int), st) != cudaSuccess) return -2;
+  if (cudaMemsetAsync(d->tile_cnt, 0, d->ntiles * sizeof(int), st) != cudaSuccess) return -2;
   if (cudaMemsetAsync(d->tile_slot[c], 0xff, d->ntiles * sizeof(int), st) != cudaSuccess) return -2;
   const long S = d->S;
   const unsigned nb = (unsigned)((S + 127) / 128);
-  lbib_node_prep<<<nb, 128, 0, st>>>(d->nodes, S, d->nx, d->ny, d->nz, d->ntx, d->nty, d->W, d->st, d->tile_flag,
+  lbib_node_prep<<<nb, 128, 0, st>>>(d->nodes, S, d->nx, d->ny, d->nz, d->ntx, d->nty, d->W, d->st, d->tile_cnt,
                                      d->chunk_box, d->err, step);
   const unsigned nblk = (unsigned)((d->ntiles + kScanBlock - 1) / kScanBlock);
-  lbib_compact_count<<<nblk, kScanBlock, 0, st>>>(d->tile_flag, d->ntiles, d->scan_tmp);
-  lbib_compact_scan<<<1, kScanBlock, 0, st>>>(d->scan_tmp, (int)nblk, d->tile_count[c]);
-  lbib_compact_write<<<nblk, kScanBlock, 0, st>>>(d->tile_flag, d->ntiles, d->scan_tmp, d->tile_list[c],
-                                                  d->tile_slot[c]);
-  lbib_spread_gather<<<148 * 8, 64, 0, st>>>(d->nodes, d->W, d->st, d->chunk_box, S, d->nchunks, d->tile_list[c],
-                                             d->tile_count[c], d->ntx, d->nty, d->Ftile[c], d->err);
-  d->kernel_launches += 5;
+  int* block_tiles = d->scan_tmp;
+  int* block_pairs = d->scan_tmp + nblk + 1;
+  lbib_compact_count<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, block_tiles, block_pairs);
+  lbib_compact_scan<<<1, kScanBlock, 0, st>>>(block_tiles, block_pairs, (int)nblk, d->tile_count[c]);
+  lbib_compact_write<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, block_tiles, block_pairs, d->tile_list[c],
+                                                  d->tile_slot[c], d->slot_off, d->slot_len, d->slot_cursor);
+  lbib_pair_scatter<<<nb, 128, 0, st>>>(d->st, S, d->ntx, d->nty, d->nx, d->ny, d->nz, d->tile_slot[c], d->slot_off,
+                                        d->slot_cursor, d->pair_node, d->err);
+  lbib_spread_gather<<<148 * 16, 64, 0, st>>>(d->nodes, d->W, d->st, d->tile_list[c], d->tile_count[c], d->slot_off,
+                                              d->slot_len, d->pair_node, d->ntx, d->nty, d->Ftile[c], d->err);
+  lbib_spread_gather_scan<<<148 * 4, 64, 0, st>>>(d->nodes, d->W, d->st, d->chunk_box, S, d->nchunks,
+                                                  d->tile_list[c], d->tile_count[c], d->slot_len, d->ntx, d->nty,
+                                                  d->Ftile[c], d->err);
+  d->kernel_launches += 7;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

@@ -55,12 +55,19 @@ typedef struct lbib_device {
   double* outlet;
   int parity;
   long steps;                    /* fused steps since init_df1               */
+  int use_bulk;                  /* staged kernel for rows away from walls   */
+  int* rows;                     /* device int2 (y, z) rows of the generic kernel */
+  int nrows;
   int have_eq, have_df1, have_inout;
   /* force / moment tiles, double buffered by step */
   int ntx, nty, ntz;
   long ntiles;
   long cap;                      /* slots per buffer                          */
-  int* tile_flag;                /* [ntiles] scratch                          */
+  int* tile_cnt;                 /* [ntiles] nodes whose stencil touches it   */
+  int* slot_off;                 /* [cap] start of the slot's node list       */
+  int* slot_len;                 /* [cap] length of the slot's node list      */
+  int* slot_cursor;              /* [cap] fill cursor                         */
+  int* pair_node;                /* [8 S] node lists of the touched tiles     */
   int* tile_slot[2];             /* [ntiles] slot or -1                       */
   int* tile_list[2];             /* [cap] touched tiles in index order        */
   int* tile_count[2];            /* [1]                                       */
@@ -75,6 +82,7 @@ typedef struct lbib_device {
   long S;
   lbib_sheet_dev* sh;            /* host array [nsheets]                      */
   double* nodes;                 /* [S][12]                                   */
+  double* h_nodes;               /* [S][12] pinned host staging for syncs     */
   double* W;                     /* [S][12]                                   */
   int* st;                       /* [S][3]                                    */
   int* chunk_box;                /* [nchunks][6]                              */

@@ -186,37 +186,63 @@ __device__ __forceinline__ void velocity_dots(double ux, double uy, double uz, d
  * and BGK relaxation, in place on f.  With a force the Guo term is added as
  * written there (true divisions by cs^2 and cs^4); without one that term is
  * +-0 in the reference and is skipped. */
+/* Guo forcing term of direction q as lbm_ib.c:1740-1754 writes it. */
+__device__ __forceinline__ double guo(int q, double ux, double uy, double uz, double Fx, double Fy, double Fzg,
+                                      const FluidParams& p) {
+  const double c0 = (double)cx(q), c1 = (double)cy(q), c2 = (double)cz(q);
+  const double kw = (q == 0) ? p.kw0 : ((q <= 6) ? p.kw1 : p.kw2);
+  const double A = (c0 - ux) * Fx + (c1 - uy) * Fy + (c2 - uz) * Fzg;
+  const double B = c0 * ux + c1 * uy + c2 * uz;
+  const double C = c0 * Fx + c1 * Fy + c2 * Fzg;
+  return kw * (A / p.cs2 + B / p.cs4 * C);
+}
+
+struct Relax {
+  double ux, uy, uz, Fx, Fy, Fzg, t6, om, it;
+};
+
+/* One opposite pair (qa, qb) with c_qa . u = cu: both equilibria share
+ * 3cu, cu^2 and 1.5 u^2, and 1 + (-3cu) == 1 - 3cu exactly.  With a force
+ * the Guo term is added after the relaxation, as the reference sums it. */
+template <bool FORCED, int QA, int QB>
+__device__ __forceinline__ void relax_pair(double* f, double cu, double wr, const Relax& r, const FluidParams& p) {
+  const double a3 = 3.0 * cu;
+  const double sq = 4.5 * (cu * cu);
+  const double ea = wr * (1.0 + a3 + sq - r.t6);
+  const double eb = wr * (1.0 + (-a3) + sq - r.t6);
+  double va = f[QA] * r.om + r.it * ea;
+  double vb = f[QB] * r.om + r.it * eb;
+  if (FORCED) {
+    va = va + guo(QA, r.ux, r.uy, r.uz, r.Fx, r.Fy, r.Fzg, p);
+    vb = vb + guo(QB, r.ux, r.uy, r.uz, r.Fx, r.Fy, r.Fzg, p);
+  }
+  f[QA] = va;
+  f[QB] = vb;
+}
+
 template <bool FORCED>
 __device__ __forceinline__ void collide(double f[19], double rho, double ux, double uy, double uz,
                                         double Fx, double Fy, double Fz, const FluidParams& p) {
-  const double usq = ux * ux + uy * uy + uz * uz;
-  const double t6 = 1.5 * usq;
+  Relax r;
+  r.ux = ux; r.uy = uy; r.uz = uz;
+  r.Fx = Fx; r.Fy = Fy; r.Fzg = FORCED ? Fz + rho * p.g : 0.0;
+  r.t6 = 1.5 * (ux * ux + uy * uy + uz * uz);
+  r.om = p.omtau; r.it = p.invtau;
   const double wr0 = 1.0 / 3.0 * rho;
   const double wr1 = 1.0 / 18.0 * rho;
   const double wr2 = 1.0 / 36.0 * rho;
-  double cu[19];
-  velocity_dots(ux, uy, uz, cu);
-  const double Fzg = Fz + rho * p.g;
-#pragma unroll
-  for (int q = 0; q < 19; ++q) {
-    double feq;
-    if (q == 0) {
-      feq = wr0 * (1.0 - t6);
-    } else {
-      const double wr = (q <= 6) ? wr1 : wr2;
-      feq = wr * (1.0 + 3.0 * cu[q] + 4.5 * (cu[q] * cu[q]) - t6);
-    }
-    double v = f[q] * p.omtau + p.invtau * feq;
-    if (FORCED) {
-      const double c0 = (double)cx(q), c1 = (double)cy(q), c2 = (double)cz(q);
-      const double kw = (q == 0) ? p.kw0 : ((q <= 6) ? p.kw1 : p.kw2);
-      const double A = (c0 - ux) * Fx + (c1 - uy) * Fy + (c2 - uz) * Fzg;
-      const double B = c0 * ux + c1 * uy + c2 * uz;
-      const double C = c0 * Fx + c1 * Fy + c2 * Fzg;
-      v = v + kw * (A / p.cs2 + B / p.cs4 * C);
-    }
-    f[q] = v;
-  }
+  double v0 = f[0] * r.om + r.it * (wr0 * (1.0 - r.t6));
+  if (FORCED) v0 = v0 + guo(0, ux, uy, uz, Fx, Fy, r.Fzg, p);
+  f[0] = v0;
+  relax_pair<FORCED, 1, 2>(f, ux, wr1, r, p);
+  relax_pair<FORCED, 3, 4>(f, uz, wr1, r, p);
+  relax_pair<FORCED, 6, 5>(f, uy, wr1, r, p);
+  relax_pair<FORCED, 7, 8>(f, ux + uz, wr2, r, p);
+  relax_pair<FORCED, 9, 10>(f, ux - uz, wr2, r, p);
+  relax_pair<FORCED, 11, 12>(f, uz - uy, wr2, r, p);
+  relax_pair<FORCED, 13, 14>(f, uy + uz, wr2, r, p);
+  relax_pair<FORCED, 15, 16>(f, ux - uy, wr2, r, p);
+  relax_pair<FORCED, 17, 18>(f, ux + uy, wr2, r, p);
 }
 
 __device__ __forceinline__ int tile_of(int x, int y, int z, int ntx, int nty) {

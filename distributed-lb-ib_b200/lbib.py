@@ -16,7 +16,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liblbib.so")
+LIB_PATH = os.environ.get("LBIB_LIBRARY") or os.path.join(HERE, "liblbib.so")
 
 COMPAT_BEND_X_BUG = 1
 COMPAT_YWALL_CUBES_X = 2

@@ -59,8 +59,19 @@ EXTRA_CASES = {
 }
 
 
+@pytest.fixture(params=["staged", "generic"])
+def fluid_path(request, monkeypatch):
+    """Rows away from the walls run the bulk-copy staged kernel unless
+    LBIB_FLUID_BULK=0; both paths must give the same bits."""
+    if request.param == "generic":
+        monkeypatch.setenv("LBIB_FLUID_BULK", "0")
+    else:
+        monkeypatch.delenv("LBIB_FLUID_BULK", raising=False)
+    return request.param
+
+
 @pytest.mark.parametrize("name", list(SMALL_CASES) + list(EXTRA_CASES))
-def test_bitexact_vs_oracle_cr(gpu, oracle_built, name):
+def test_bitexact_vs_oracle_cr(gpu, oracle_built, fluid_path, name):
     case, steps = {**SMALL_CASES, **EXTRA_CASES}[name]
     s = lbib.Solver(case)
     o = P.Oracle(case, cr_cos=True)
