@@ -36,6 +36,7 @@ const char* lbib_error_string(int code) {
     case LBIB_E_NOMEM: return "allocation failed";
     case LBIB_E_CAPACITY: return "touched-tile capacity exceeded";
     case LBIB_E_IO: return "a dump file could not be written";
+    case LBIB_E_LIMIT: return "size above the fixed maximum of the no-allocation entry point";
     default: return "unknown error";
   }
 }

@@ -165,6 +165,7 @@ typedef struct lv_t {
 #define LBIB_E_NOMEM        -5   /* device or host allocation failed         */
 #define LBIB_E_CAPACITY     -6   /* more touched force tiles than allocated  */
 #define LBIB_E_IO           -7   /* a dump file could not be written         */
+#define LBIB_E_LIMIT        -8   /* a size above a fixed maximum             */
 
 /* ---- set-up: mpi/init_gv.c, mpi/gen_*.c, mpi/init_*.c ----------------- */
 
@@ -289,6 +290,37 @@ void lbib_case_free(GV gv);
  * 4 compute_eqlbrmdistrfuncDF1, 5 stream, 6 bounce-back, 7 rho and u,
  * 8 interpolate and move, 9 inlet/outlet copy, 10 replace_old_DF. */
 int lbib_stage(GV gv, int which);
+
+/* ---- force spreading without allocation (no counterpart in the
+ * reference) ------------------------------------------------------------
+ *
+ * For hosts that cannot allocate GPU memory while they run -- e.g. a host
+ * that hands out buffers from its own fixed pool and forbids any cudaMalloc
+ * after start-up, because allocation may synchronise the device or fail
+ * under its memory cap.  The GV path allocates its tile lists, maps and
+ * weights when a sheet is uploaded; this entry point allocates nothing.
+ *
+ * Computes the spread force F of fiber_SpreadForce + fluid_get_SpreadForce
+ * (cube_pthread/lbm_ib.c:1323-1525) from `nodes`, num_nodes Fibernode
+ * records (12 doubles each, all sheets concatenated in sheet, row, col
+ * order; only x, y, z and the elastic force are read), into fx, fy, fz
+ * (nx*ny*nz doubles each, x fastest), all device pointers owned by the
+ * caller; the result equals the GV path's bit for bit.  Runs on `stream`
+ * (a cudaStream_t, NULL for the default stream) and waits for it before
+ * returning.  Returns LBIB_OK, LBIB_E_STENCIL (a stencil leaves the grid;
+ * outputs zero), LBIB_E_LIMIT (num_nodes > LBIB_NOALLOC_MAX_NODES) or
+ * LBIB_E_ARG / LBIB_E_CUDA.
+ *
+ * Its scratch (per 32-node chunk the stencil bounding box, the box of all
+ * stencils and an error word) is one file-scope device array of ~192 KiB,
+ * which every GPU that loads the library keeps until the process exits.
+ * The first call on each device looks up that array's device address with
+ * the device current; make that first call before any stream capture.  All
+ * calls share the array: calls whose work overlaps on the GPU (other
+ * streams, other host threads on the same device) race -- serialise them. */
+#define LBIB_NOALLOC_MAX_NODES (1 << 18)
+int lbib_spread_force_noalloc(const double* nodes, long num_nodes, int nx, int ny, int nz,
+                              double* fx, double* fy, double* fz, void* stream);
 
 #ifdef __cplusplus
 }
