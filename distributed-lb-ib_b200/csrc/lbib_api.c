@@ -82,6 +82,7 @@ void init_gv_constant(GV gv) {
   gv->Ks_l = gv->Kshat * gv->rho_l * gv->u_l * gv->u_l * gv->L_l;
   memcpy(gv->c, LBIB_C, sizeof(LBIB_C));
   gv->lbib_compat = LBIB_COMPAT_ALL;
+  gv->lbib_precision = LBIB_PREC_F64;
 }
 
 static void fill_config(GV gv, lbdev_config* c) {
@@ -90,6 +91,7 @@ static void fill_config(GV gv, lbdev_config* c) {
   c->nz = gv->fluid_grid->z_dim;
   c->cube_size = gv->cube_size;
   c->compat = gv->lbib_compat;
+  c->prec = gv->lbib_precision;
   c->tau = gv->tau; c->u_l = gv->u_l; c->rho_l = gv->rho_l;
   c->Ks_l = gv->Ks_l; c->Kb_l = gv->Kb_l; c->g_l = gv->g_l; c->cs_l = gv->cs_l;
   c->dt = gv->dt;
@@ -239,6 +241,26 @@ int lbib_set_compat(GV gv, int flags) {
     lbdev_config c;
     fill_config(gv, &c);
     lbdev_set_physics(gv->dev, &c);
+  }
+  return LBIB_OK;
+}
+
+static int precision_ok(int p) {
+  const int t = p & ~LBIB_PREC_SHIFT_FLOW;
+  return t >= LBIB_PREC_F32 && t <= LBIB_PREC_BF16 ? 1 : p == LBIB_PREC_F64;
+}
+
+int lbib_set_precision(GV gv, int precision) {
+  if (!gv || !precision_ok(precision)) return set_error(LBIB_E_ARG);
+  if (gv->dev && gv->dev->S > 0) return set_error(LBIB_E_STATE);
+  gv->lbib_precision = precision;
+  if (gv->dev && gv->dev->prec != precision) {
+    lbdev_free(gv->dev);
+    gv->dev = NULL;
+    lbdev_config c;
+    fill_config(gv, &c);
+    int rc = lbdev_create(&gv->dev, &c);
+    if (rc) return set_error(rc);
   }
   return LBIB_OK;
 }
@@ -407,6 +429,13 @@ int lbib_get_force(GV gv, double* fx, double* fy, double* fz) {
   return rc ? set_error(rc) : LBIB_OK;
 }
 
+int lbib_conservation_sums(GV gv, double* out) {
+  if (!gv || !out) return set_error(LBIB_E_ARG);
+  if (!gv->dev) return set_error(LBIB_E_STATE);
+  int rc = lbdev_conservation(gv->dev, out);
+  return rc ? set_error(rc) : LBIB_OK;
+}
+
 int lbib_get_df1(GV gv, double* out) {
   if (!gv || !gv->dev) return set_error(LBIB_E_STATE);
   if (!out) return set_error(LBIB_E_ARG);
@@ -459,7 +488,18 @@ GV lbib_case_create(int nx, int ny, int nz, int cube_size, int nsheets,
                     const double* width, const double* height,
                     const double* x0, const double* y0, const double* z0,
                     double tau, double u_l, double Ks_l, double Kb_l, int compat) {
-  if (nsheets < 1 || !rows || !cols || !width || !height || !x0 || !y0 || !z0) {
+  return lbib_case_create_prec(nx, ny, nz, cube_size, nsheets, rows, cols, width, height, x0, y0, z0,
+                               tau, u_l, Ks_l, Kb_l, compat, LBIB_PREC_F64);
+}
+
+GV lbib_case_create_prec(int nx, int ny, int nz, int cube_size, int nsheets,
+                         const int* rows, const int* cols,
+                         const double* width, const double* height,
+                         const double* x0, const double* y0, const double* z0,
+                         double tau, double u_l, double Ks_l, double Kb_l, int compat,
+                         int precision) {
+  if (nsheets < 1 || !rows || !cols || !width || !height || !x0 || !y0 || !z0 ||
+      !precision_ok(precision)) {
     set_error(LBIB_E_ARG);
     return NULL;
   }
@@ -481,6 +521,7 @@ GV lbib_case_create(int nx, int ny, int nz, int cube_size, int nsheets,
   int before = lbib_last_error();
   init_gv_constant(gv);
   gv->lbib_compat = compat;
+  gv->lbib_precision = precision;
   gv->tau = tau; gv->u_l = u_l; gv->Ks_l = Ks_l; gv->Kb_l = Kb_l;
   gen_fluid_grid(gv->fluid_grid, cube_size, 0, gv);
   for (int k = 0; k < nsheets; ++k) gen_fiber_sheet(&gv->fiber_shape->sheets[k]);

@@ -17,7 +17,8 @@ int lbdev_launch_fluid_step(lbib_device* d);
 int lbdev_launch_tile_moments(lbib_device* d);
 int lbdev_launch_field_moments(lbib_device* d, double* rho, double* ux, double* uy, double* uz);
 int lbdev_launch_gather_df1(lbib_device* d, double* out);
-int lbdev_launch_init_eq(lbib_device* d, double* f, long count, long stride);
+int lbdev_launch_init(lbib_device* d, int what);
+int lbdev_launch_sums(lbib_device* d, double* part, double* out);
 int lbdev_launch_fiber_forces(lbib_device* d, int k);
 int lbdev_launch_spread(lbib_device* d, int step);
 int lbdev_launch_move(lbib_device* d);
@@ -89,13 +90,41 @@ static void derive_boundaries(lbib_device* d) {
 
 extern "C" int lbdev_bulk_rows(const lbib_device* d, int* nrows_y, int* nrows_z);
 
+/* Bytes of one stored population value. */
+extern "C" size_t lbdev_pop_bytes(int prec) {
+  const int t = LBIB_PREC_TYPE(prec);
+  return t == LBIB_PREC_F64 ? 8 : t == LBIB_PREC_F32 ? 4 : 2;
+}
+
+/* Shift of the low-precision forms: the rest weights w_q (rho_s = 1,
+ * u_s = 0), or with LBIB_PREC_SHIFT_FLOW the equilibrium of the initial
+ * state (rho_l, u_l, 0, 0), which the inflow keeps the bulk of the grid near. */
+extern "C" void lbdev_shift(const lbib_device* d, float* sh, double* rhos, double* uxs) {
+  if (LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64) {
+    for (int q = 0; q < 19; ++q) sh[q] = 0.0f;
+    *rhos = 0.0; *uxs = 0.0;
+    return;
+  }
+  const int flow = (d->prec & LBIB_PREC_SHIFT_FLOW) != 0;
+  const double rho = flow ? d->rho_l : 1.0, ux = flow ? d->u_l : 0.0;
+  static const int cxq[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+  for (int q = 0; q < 19; ++q) {
+    const double w = q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
+    const double cu = cxq[q] * ux;
+    sh[q] = (float)(w * rho * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * ux * ux));
+  }
+  *rhos = rho;
+  *uxs = ux;
+}
+
 /* Rows (y, z) of I that the generic fused kernel processes: all of them, or,
  * with the staged kernel on, those it does not take (next to the walls, or
  * above zin_hi).  The staged kernel needs even nx for aligned copies. */
 static int build_rows(lbib_device* d) {
   const char* env = getenv("LBIB_FLUID_BULK");
   int ry = 0, rz = 0;
-  d->use_bulk = !(env && env[0] == '0') && (d->nx % 2 == 0) && lbdev_bulk_rows(d, &ry, &rz);
+  d->use_bulk = !(env && env[0] == '0') && LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 && (d->nx % 2 == 0) &&
+                lbdev_bulk_rows(d, &ry, &rz);
   const int zb = 2 + rz;  /* last z row of the staged kernel */
   long cap = (long)(d->ny - 4) * (d->nz - 4);
   int* h = (int*)malloc(sizeof(int) * 2 * cap);
@@ -133,6 +162,7 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   lbib_device* d = (lbib_device*)calloc(1, sizeof(lbib_device));
   if (!d) return -5;
   d->nx = c->nx; d->ny = c->ny; d->nz = c->nz;
+  d->prec = c->prec;
   d->N = (long)c->nx * c->ny * c->nz;
   d->cube_size = c->cube_size;
   d->ncx = c->nx / c->cube_size; d->ncy = c->ny / c->cube_size; d->ncz = c->nz / c->cube_size;
@@ -142,14 +172,15 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   d->ntx = (d->nx + 3) / 4; d->nty = (d->ny + 3) / 4; d->ntz = (d->nz + 3) / 4;
   d->ntiles = (long)d->ntx * d->nty * d->ntz;
   int rc = 0;
-  if (cudaMalloc(&d->f, sizeof(double) * 19 * d->N) != cudaSuccess) rc = -5;
+  const size_t pop = lbdev_pop_bytes(d->prec), real = LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 ? 8 : 4;
+  if (cudaMalloc(&d->f, pop * 19 * d->N) != cudaSuccess) rc = -5;
   long P = (long)d->ny * d->nz;
-  if (!rc && cudaMalloc(&d->inlet, sizeof(double) * 19 * P) != cudaSuccess) rc = -5;
-  if (!rc && cudaMalloc(&d->outlet, sizeof(double) * 19 * P) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&d->inlet, real * 19 * P) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&d->outlet, real * 19 * P) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&d->err, sizeof(int) * 2) != cudaSuccess) rc = -5;
   if (!rc && cudaMallocHost(&d->h_err, sizeof(int) * 2) != cudaSuccess) rc = -5;
   if (!rc && cudaMemsetAsync(d->err, 0, sizeof(int) * 2, d->stream) != cudaSuccess) rc = -2;
-  if (!rc && cudaMemsetAsync(d->f, 0, sizeof(double) * 19 * d->N, d->stream) != cudaSuccess) rc = -2;
+  if (!rc && cudaMemsetAsync(d->f, 0, pop * 19 * d->N, d->stream) != cudaSuccess) rc = -2;
   if (!rc) rc = build_rows(d);
   if (rc) { lbdev_free(d); return rc; }
   d->cur = 0;
@@ -230,7 +261,7 @@ extern "C" int lbdev_init_equilibrium(lbib_device* d) {
 }
 
 extern "C" int lbdev_init_df1(lbib_device* d) {
-  if (lbdev_launch_init_eq(d, d->f, d->N, d->N)) return -2;
+  if (lbdev_launch_init(d, 0)) return -2;
   d->parity = 0;
   d->steps = 0;
   d->have_df1 = 1;
@@ -242,9 +273,7 @@ extern "C" int lbdev_init_df1(lbib_device* d) {
 }
 
 extern "C" int lbdev_init_inout(lbib_device* d) {
-  long P = (long)d->ny * d->nz;
-  if (lbdev_launch_init_eq(d, d->inlet, P, P)) return -2;
-  if (lbdev_launch_init_eq(d, d->outlet, P, P)) return -2;
+  if (lbdev_launch_init(d, 1)) return -2;
   d->have_inout = 1;
   return 0;
 }
@@ -399,6 +428,20 @@ extern "C" int lbdev_get_df1(lbib_device* d, double* out) {
   CK(cudaMemsetAsync(s, 0, sizeof(double) * 19 * N, d->stream));
   if (lbdev_launch_gather_df1(d, s)) return -2;
   CK(cudaMemcpyAsync(out, s, sizeof(double) * 19 * N, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  cudaFree(d->scratch);
+  d->scratch = NULL;
+  return 0;
+}
+
+/* out[4] = FP64 mass and x, y, z momentum of the populations of I. */
+extern "C" int lbdev_conservation(lbib_device* d, double* out) {
+  if (!d->have_df1) return -4;
+  const long rows = (long)(d->ny - 4) * (d->nz - 4);
+  if (ensure_scratch(d, 4 * rows + 4)) return -5;
+  double* s = d->scratch;
+  if (lbdev_launch_sums(d, s + 4, s)) return -2;
+  CK(cudaMemcpyAsync(out, s, sizeof(double) * 4, cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));
   cudaFree(d->scratch);
   d->scratch = NULL;

@@ -1,0 +1,447 @@
+/*
+ * Fluid kernels, templated on the population storage type T (double, float,
+ * __half, __nv_bfloat16; arithmetic in Pop<T>::R), and their launchers.
+ *
+ * lbib_fluid_step<T, PAR> replaces, for one time step, the reference's
+ * compute_eqlbrmdistrfuncDF1 + stream_distrfunc + bounceback_rigidwalls +
+ * copy_inout_to_df2 + replace_old_DF (cube_pthread/lbm_ib.c:1673-2968):
+ * each cell of I reads its 19 incoming populations once and writes its 19
+ * outgoing ones once (AA pattern, one buffer).  It needs the previous step's
+ * moments: cells whose 4^3 tile carried force last step read them from the
+ * stored tile moments; every other cell recomputes them from its incoming
+ * populations, which is exact because F(t-1) = 0 there.
+ *
+ * HBM roofline: 2 x 19 x sizeof(T) bytes per fluid cell (304 B for FP64,
+ * 76 B for the 16-bit forms).
+ *
+ * lbib_fluid.cu instantiates T = double in a translation unit compiled with
+ * -fmad=false (bit-faithful to the reference); lbib_fluid_lp.cu instantiates
+ * the other types with contraction allowed.
+ */
+#ifndef LBIB_FLUID_KERNELS_CUH
+#define LBIB_FLUID_KERNELS_CUH
+
+#include "lbib_internal.h"
+#include "lbib_lattice.cuh"
+
+namespace lbib {
+
+/* Resident blocks per SM the register budget is sized for (128 threads each). */
+#ifndef LBIB_FLUID_MINB
+#define LBIB_FLUID_MINB 4
+#endif
+
+/* The equilibrium of the initial (rho_l, u_l, 0, 0), as
+ * init_eqlbrmdistrfuncDF0 writes it (lbm_ib.c:1528-1607). */
+template <typename R>
+__host__ __device__ __forceinline__ R init_feq(int q, R rho, R ux) {
+  const R uy = R(0), uz = R(0);
+  const R usq = ux * ux + uy * uy + uz * uz;
+  const R t6 = R(1.5) * usq;
+  if (q == 0) return R(1.0 / 3.0) * rho * (R(1.0) - t6);
+  const R cu = (R)cx(q) * ux;
+  return R((q <= 6) ? 1.0 / 18.0 : 1.0 / 36.0) * rho * (R(1.0) + R(3.0) * cu + R(4.5) * (cu * cu) - t6);
+}
+
+/* Moments of a cell in the form its collision takes. */
+template <typename R>
+struct Mom {
+  R rho, ux, uy, uz;
+};
+
+/* Deviation-form BGK + Guo for one opposite pair (qa, qb), c_qa = -c_qb:
+ *   a = c.u, a0 = c.u_s, da = c.(u - u_s),
+ *   P(u) = 3a + 4.5 a^2 - 1.5 u^2,
+ *   feq - s = w (drho (1 + P(u)) + rho_s (P(u) - P(u_s))),
+ *   P(u) - P(u_s) = 3 da + 4.5 da (a + a0) - 1.5 (u - u_s).(u + u_s),
+ * so every term is a small number and FP32 keeps its digits. */
+template <bool FORCED, int QA, int QB, typename P>
+__device__ __forceinline__ void lp_relax_pair(float* d, float a, float da, float a0, float w, float drho,
+                                              float rs, float t, float td, float om, float it, float ux,
+                                              float uy, float uz, float Fx, float Fy, float Fzg, const P& p) {
+  const float sq = 4.5f * a * a - t;
+  const float dq = 4.5f * da * (a + a0) - td;
+  const float ea = w * (drho * (1.0f + sq + 3.0f * a) + rs * (dq + 3.0f * da));
+  const float eb = w * (drho * (1.0f + sq - 3.0f * a) + rs * (dq - 3.0f * da));
+  float va = d[QA] * om + it * ea;
+  float vb = d[QB] * om + it * eb;
+  if (FORCED) {
+    va += guo(QA, ux, uy, uz, Fx, Fy, Fzg, p);
+    vb += guo(QB, ux, uy, uz, Fx, Fy, Fzg, p);
+  }
+  d[QA] = va;
+  d[QB] = vb;
+}
+
+/* Form<T>: how the kernels turn populations into moments and collide.
+ * FP64: absolute (rho, u) and the reference's own arithmetic.  The
+ * low-precision forms: deviations d_q = f_q - s_q, drho = rho - rho_s,
+ * du = u - u_s (u_s = (uxs, 0, 0)), all in FP32. */
+template <typename T, bool LOW = (sizeof(T) < 8)>
+struct Form;
+
+template <typename T>
+struct Form<T, false> {
+  using R = double;
+  using P = FluidParamsT<T>;
+  static __device__ __forceinline__ void initial(const P& p, Mom<R>& m) {
+    m.rho = p.rho0; m.ux = p.ux0; m.uy = 0.0; m.uz = 0.0;
+  }
+  static __device__ __forceinline__ void from_tile(const P&, const double* U, int cell, Mom<R>& m) {
+    m.rho = U[cell]; m.ux = U[64 + cell]; m.uy = U[128 + cell]; m.uz = U[192 + cell];
+  }
+  static __device__ __forceinline__ void moments(const R f[19], R Fx, R Fy, R Fz, const P& p, Mom<R>& m) {
+    lbib::moments(f, Fx, Fy, Fz, p.half_dt, p.g, m.rho, m.ux, m.uy, m.uz);
+  }
+  template <bool FORCED>
+  static __device__ __forceinline__ void collide(R f[19], const Mom<R>& m, R Fx, R Fy, R Fz, const P& p) {
+    lbib::collide<FORCED>(f, m.rho, m.ux, m.uy, m.uz, Fx, Fy, Fz, p);
+  }
+  static __device__ __forceinline__ void to_double(const Mom<R>& m, const P&, double& rho, double& ux,
+                                                   double& uy, double& uz) {
+    rho = m.rho; ux = m.ux; uy = m.uy; uz = m.uz;
+  }
+  static __device__ __forceinline__ double value(R v, int, const P&) { return v; }
+  static __device__ __forceinline__ R stored_initial(int q, double rho, double ux, const P&) {
+    return init_feq<double>(q, rho, ux);
+  }
+};
+
+template <typename T>
+struct Form<T, true> {
+  using R = float;
+  using P = FluidParamsT<T>;
+  static __device__ __forceinline__ void initial(const P& p, Mom<R>& m) {
+    m.rho = (float)(p.rho0 - p.rhos); m.ux = (float)(p.ux0 - p.uxs); m.uy = 0.0f; m.uz = 0.0f;
+  }
+  static __device__ __forceinline__ void from_tile(const P& p, const double* U, int cell, Mom<R>& m) {
+    m.rho = (float)(U[cell] - p.rhos); m.ux = (float)(U[64 + cell] - p.uxs);
+    m.uy = (float)U[128 + cell]; m.uz = (float)U[192 + cell];
+  }
+  static __device__ __forceinline__ void moments(const R d[19], R Fx, R Fy, R Fz, const P& p, Mom<R>& m) {
+    /* pairwise sums: short dependency chains, small magnitudes */
+    const float m0 = ((d[0] + d[1]) + (d[2] + d[3])) + ((d[4] + d[5]) + (d[6] + d[7]));
+    const float m1 = ((d[8] + d[9]) + (d[10] + d[11])) + ((d[12] + d[13]) + (d[14] + d[15]));
+    const float drho = (m0 + m1) + ((d[16] + d[17]) + d[18]);
+    const float jx = ((d[1] - d[2]) + (d[7] - d[8])) + ((d[9] - d[10]) + (d[15] - d[16])) + (d[17] - d[18]);
+    const float jy = ((d[6] - d[5]) + (d[12] - d[11])) + ((d[13] - d[14]) + (d[16] - d[15])) + (d[17] - d[18]);
+    const float jz = ((d[3] - d[4]) + (d[7] - d[8])) + ((d[10] - d[9]) + (d[11] - d[12])) + (d[13] - d[14]);
+    const float rs = (float)p.rhos, us = (float)p.uxs, h = (float)p.half_dt;
+    const float rho = rs + drho;
+    const float inv = 1.0f / rho;
+    m.rho = drho;
+    m.ux = (jx + h * Fx - drho * us) * inv;
+    m.uy = (jy + h * Fy) * inv;
+    m.uz = (jz + h * (Fz + rho * (float)p.g)) * inv;
+  }
+  template <bool FORCED>
+  static __device__ __forceinline__ void collide(R d[19], const Mom<R>& m, R Fx, R Fy, R Fz, const P& p) {
+    const float rs = (float)p.rhos, us = (float)p.uxs;
+    const float drho = m.rho, dux = m.ux, duy = m.uy, duz = m.uz;
+    const float ux = us + dux, uy = duy, uz = duz;
+    const float rho = rs + drho;
+    const float t = 1.5f * (ux * ux + uy * uy + uz * uz);
+    const float td = 1.5f * (dux * (ux + us) + duy * uy + duz * uz);
+    const float om = (float)p.omtau, it = (float)p.invtau;
+    const float Fzg = FORCED ? Fz + rho * (float)p.g : 0.0f;
+    const float w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
+    float v0 = d[0] * om + it * ((1.0f / 3.0f) * (drho * (1.0f - t) - rs * td));
+    if (FORCED) v0 += guo(0, ux, uy, uz, Fx, Fy, Fzg, p);
+    d[0] = v0;
+    lp_relax_pair<FORCED, 1, 2>(d, ux, dux, us, w1, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_relax_pair<FORCED, 3, 4>(d, uz, duz, 0.0f, w1, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_relax_pair<FORCED, 6, 5>(d, uy, duy, 0.0f, w1, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_relax_pair<FORCED, 7, 8>(d, ux + uz, dux + duz, us, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_relax_pair<FORCED, 9, 10>(d, ux - uz, dux - duz, us, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_relax_pair<FORCED, 11, 12>(d, uz - uy, duz - duy, 0.0f, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_relax_pair<FORCED, 13, 14>(d, uy + uz, duy + duz, 0.0f, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_relax_pair<FORCED, 15, 16>(d, ux - uy, dux - duy, us, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_relax_pair<FORCED, 17, 18>(d, ux + uy, dux + duy, us, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+  }
+  static __device__ __forceinline__ void to_double(const Mom<R>& m, const P& p, double& rho, double& ux,
+                                                   double& uy, double& uz) {
+    rho = p.rhos + (double)m.rho; ux = p.uxs + (double)m.ux; uy = m.uy; uz = m.uz;
+  }
+  static __device__ __forceinline__ double value(R v, int q, const P& p) { return (double)p.sh[q] + (double)v; }
+  static __device__ __forceinline__ R stored_initial(int q, double rho, double ux, const P& p) {
+    return (float)(init_feq<double>(q, rho, ux) - (double)p.sh[q]);
+  }
+};
+
+template <typename T, int PAR>
+__global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
+    lbib_fluid_step(FluidParamsT<T> p, const int2* __restrict__ rows) {
+  using R = typename Pop<T>::R;
+  const int x = blockIdx.y * blockDim.x + threadIdx.x + 2;
+  const int2 r = rows[blockIdx.x];
+  const int y = r.x;
+  const int z = r.y;
+  if (x > p.nx - 3) return;
+  const long idx = ((long)z * p.ny + y) * p.nx + x;
+  const int kind = classify(p, x, y, z);
+  R f[19];
+  load_pre<PAR>(p, x, y, z, idx, kind, f);
+  const int tile = tile_of(x, y, z, p.ntx, p.nty);
+  const int cell = cell_in_tile(x, y, z);
+  using F = Form<T>;
+  Mom<R> m;
+  if (kind >= K_SEMI || p.first) {
+    F::initial(p, m);
+  } else {
+    const int sp = p.slot_prev[tile];
+    if (sp >= 0) F::from_tile(p, p.Uprev + (long)sp * 256, cell, m);
+    else F::moments(f, R(0), R(0), R(0), p, m);
+  }
+  const int sc = p.slot_cur[tile];
+  if (sc >= 0) {
+    const double* Ft = p.Fcur + (long)sc * 192;
+    F::template collide<true>(f, m, (R)Ft[cell], (R)Ft[64 + cell], (R)Ft[128 + cell], p);
+  } else {
+    F::template collide<false>(f, m, R(0), R(0), R(0), p);
+  }
+  store_post<PAR>(p, x, y, z, idx, kind, f);
+}
+
+/* (rho, u)(t) of every cell of the touched tiles, after the fused step of
+ * parity 1-PAR: compute_rho_and_u (lbm_ib.c:2440-2538) restricted to where
+ * moveFiberSheet will read.  Cells outside M keep the initial values. */
+template <typename T, int PAR>
+__global__ void lbib_tile_moments(FluidParamsT<T> p, const int* __restrict__ list, const int* __restrict__ count,
+                                  const double* __restrict__ Ftile, double* __restrict__ Utile) {
+  using R = typename Pop<T>::R;
+  const int n = *count;
+  const int cell = threadIdx.x;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int tile = list[i];
+    const int tx = tile % p.ntx, ty = (tile / p.ntx) % p.nty, tz = tile / (p.ntx * p.nty);
+    const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
+    double rho = p.rho0, ux = p.ux0, uy = 0.0, uz = 0.0;
+    if (x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
+      const long idx = ((long)z * p.ny + y) * p.nx + x;
+      R f[19];
+      load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
+      const double* Ft = Ftile + (long)i * 192;
+      Mom<R> m;
+      Form<T>::moments(f, (R)Ft[cell], (R)Ft[64 + cell], (R)Ft[128 + cell], p, m);
+      Form<T>::to_double(m, p, rho, ux, uy, uz);
+    }
+    double* U = Utile + (long)i * 256;
+    U[cell] = rho; U[64 + cell] = ux; U[128 + cell] = uy; U[192 + cell] = uz;
+  }
+}
+
+/* Dense rho, u over the whole grid as the reference holds them after the
+ * step: M cells from the populations (with this step's force where a tile
+ * carried one), all other cells at the initial values. */
+template <typename T, int PAR>
+__global__ void lbib_field_moments(FluidParamsT<T> p, int have_step, double* __restrict__ rho_o,
+                                   double* __restrict__ ux_o, double* __restrict__ uy_o,
+                                   double* __restrict__ uz_o) {
+  using R = typename Pop<T>::R;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  if (x >= p.nx) return;
+  const long idx = ((long)z * p.ny + y) * p.nx + x;
+  double rho = p.rho0, ux = p.ux0, uy = 0.0, uz = 0.0;
+  if (have_step && x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
+    R f[19];
+    load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
+    R Fx = R(0), Fy = R(0), Fz = R(0);
+    const int sc = p.slot_cur[tile_of(x, y, z, p.ntx, p.nty)];
+    if (sc >= 0) {
+      const int cell = cell_in_tile(x, y, z);
+      const double* Ft = p.Fcur + (long)sc * 192;
+      Fx = (R)Ft[cell]; Fy = (R)Ft[64 + cell]; Fz = (R)Ft[128 + cell];
+    }
+    Mom<R> m;
+    Form<T>::moments(f, Fx, Fy, Fz, p, m);
+    Form<T>::to_double(m, p, rho, ux, uy, uz);
+  }
+  rho_o[idx] = rho; ux_o[idx] = ux; uy_o[idx] = uy; uz_o[idx] = uz;
+}
+
+/* df1 as the reference holds it at the start of the next step, for cells of
+ * I (natural layout [q][idx]); other cells are left untouched. */
+template <typename T, int PAR>
+__global__ void lbib_gather_df1(FluidParamsT<T> p, double* __restrict__ out) {
+  using R = typename Pop<T>::R;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int y = blockIdx.y + 2, z = blockIdx.z + 2;
+  if (x > p.nx - 3) return;
+  const long idx = ((long)z * p.ny + y) * p.nx + x;
+  R f[19];
+  load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
+#pragma unroll
+  for (int q = 0; q < 19; ++q) out[q * p.N + idx] = Form<T>::value(f[q], q, p);
+}
+
+/* FP64 mass and momentum of the populations of I as the next step reads
+ * them, one partial per (y, z) row.  Each block owns a row; its 128 threads
+ * stride over x and the block sum is a fixed tree, so the result does not
+ * depend on scheduling. */
+template <typename T, int PAR>
+__global__ void __launch_bounds__(128) lbib_row_sums(FluidParamsT<T> p, double* __restrict__ part) {
+  using R = typename Pop<T>::R;
+  const int y = blockIdx.x + 2, z = blockIdx.y + 2;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  for (int x = threadIdx.x + 2; x <= p.nx - 3; x += blockDim.x) {
+    const long idx = ((long)z * p.ny + y) * p.nx + x;
+    R f[19];
+    load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
+    double m = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      const double v = Form<T>::value(f[q], q, p);
+      m += v;
+      if (cx(q)) jx += cx(q) > 0 ? v : -v;
+      if (cy(q)) jy += cy(q) > 0 ? v : -v;
+      if (cz(q)) jz += cz(q) > 0 ? v : -v;
+    }
+    s0 += m; s1 += jx; s2 += jy; s3 += jz;
+  }
+  __shared__ double sh[4][128];
+  sh[0][threadIdx.x] = s0; sh[1][threadIdx.x] = s1; sh[2][threadIdx.x] = s2; sh[3][threadIdx.x] = s3;
+  __syncthreads();
+  for (int w = 64; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int k = 0; k < 4; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) part[((long)blockIdx.y * gridDim.x + blockIdx.x) * 4 + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+/* Sum of n row partials [n][4] in a fixed order: thread t adds rows t,
+ * t + 256, ... in turn, then a fixed tree. */
+static __global__ void __launch_bounds__(256) lbib_sum_rows(const double* __restrict__ part, long n, double* __restrict__ out) {
+  __shared__ double sh[4][256];
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long r = threadIdx.x; r < n; r += 256)
+    for (int k = 0; k < 4; ++k) s[k] += part[r * 4 + k];
+  for (int k = 0; k < 4; ++k) sh[k][threadIdx.x] = s[k];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int k = 0; k < 4; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = sh[threadIdx.x][0];
+}
+
+/* init_df1 (lbm_ib.c:2725-2767): every cell in natural order. */
+template <typename T>
+__global__ void lbib_init_pop(FluidParamsT<T> p, T* __restrict__ f, long count) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+#pragma unroll
+  for (int q = 0; q < 19; ++q) f[q * count + i] = Pop<T>::put(Form<T>::stored_initial(q, p.rho0, p.ux0, p));
+}
+
+/* init_df_inout (lbm_ib.c:1610-1670): the fixed inlet/outlet planes. */
+template <typename T>
+__global__ void lbib_init_table(FluidParamsT<T> p, typename Pop<T>::R* __restrict__ t, long count) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+#pragma unroll
+  for (int q = 0; q < 19; ++q) t[q * count + i] = Form<T>::stored_initial(q, p.rho0, p.ux0, p);
+}
+
+template <typename T>
+FluidParamsT<T> make_params_t(lbib_device* d, int first) {
+  using R = typename Pop<T>::R;
+  FluidParamsT<T> p;
+  p.f = (T*)d->f; p.inlet = (const R*)d->inlet; p.outlet = (const R*)d->outlet;
+  p.N = d->N; p.nx = d->nx; p.ny = d->ny; p.nz = d->nz;
+  p.zin_hi = d->zin_hi; p.yskip_z0 = d->yskip_z0; p.first = first;
+  p.rho0 = d->rho_l; p.ux0 = d->u_l;
+  p.omtau = d->omtau; p.invtau = d->invtau;
+  p.kw0 = d->kw[0]; p.kw1 = d->kw[1]; p.kw2 = d->kw[2];
+  p.cs2 = d->cs2; p.cs4 = d->cs4; p.half_dt = d->half_dt; p.g = d->g_l;
+  const int c = d->cur;
+  p.slot_cur = d->tile_slot[c]; p.Fcur = d->Ftile[c];
+  p.slot_prev = d->tile_slot[c ^ 1]; p.Uprev = d->Utile[c ^ 1];
+  p.ntx = d->ntx; p.nty = d->nty;
+  lbdev_shift(d, p.sh, &p.rhos, &p.uxs);
+  return p;
+}
+
+/* The generic kernel over d->rows. */
+template <typename T>
+int launch_step_rows_t(lbib_device* d, const FluidParamsT<T>& p) {
+  if (d->nrows <= 0) return 0;
+  dim3 block(128);
+  dim3 grid((unsigned)d->nrows, (unsigned)((d->nx - 4 + 127) / 128));
+  if (d->parity == 0) lbib_fluid_step<T, 0><<<grid, block, 0, d->stream>>>(p, (const int2*)d->rows);
+  else lbib_fluid_step<T, 1><<<grid, block, 0, d->stream>>>(p, (const int2*)d->rows);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename T>
+int launch_tile_moments_t(lbib_device* d) {
+  FluidParamsT<T> p = make_params_t<T>(d, 0);
+  const int c = d->cur;
+  const int blocks = 148 * 16;
+  if (d->parity == 0)
+    lbib_tile_moments<T, 0><<<blocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], d->Ftile[c], d->Utile[c]);
+  else
+    lbib_tile_moments<T, 1><<<blocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], d->Ftile[c], d->Utile[c]);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename T>
+int launch_field_moments_t(lbib_device* d, double* rho, double* ux, double* uy, double* uz) {
+  FluidParamsT<T> p = make_params_t<T>(d, 0);
+  dim3 block(128);
+  dim3 grid((unsigned)((d->nx + 127) / 128), (unsigned)d->ny, (unsigned)d->nz);
+  const int have = d->steps > 0 && d->have_forces;
+  if (d->parity == 0) lbib_field_moments<T, 0><<<grid, block, 0, d->stream>>>(p, have, rho, ux, uy, uz);
+  else lbib_field_moments<T, 1><<<grid, block, 0, d->stream>>>(p, have, rho, ux, uy, uz);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename T>
+int launch_gather_df1_t(lbib_device* d, double* out) {
+  FluidParamsT<T> p = make_params_t<T>(d, d->steps == 0);
+  dim3 block(128);
+  dim3 grid((unsigned)((d->nx - 4 + 127) / 128), (unsigned)(d->ny - 4), (unsigned)(d->nz - 4));
+  if (d->parity == 0) lbib_gather_df1<T, 0><<<grid, block, 0, d->stream>>>(p, out);
+  else lbib_gather_df1<T, 1><<<grid, block, 0, d->stream>>>(p, out);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+/* Mass and momentum sums into out[4] (device); part holds (ny-4)(nz-4)*4
+ * doubles. */
+template <typename T>
+int launch_sums_t(lbib_device* d, double* part, double* out) {
+  FluidParamsT<T> p = make_params_t<T>(d, d->steps == 0);
+  dim3 grid((unsigned)(d->ny - 4), (unsigned)(d->nz - 4));
+  if (d->parity == 0) lbib_row_sums<T, 0><<<grid, 128, 0, d->stream>>>(p, part);
+  else lbib_row_sums<T, 1><<<grid, 128, 0, d->stream>>>(p, part);
+  lbib_sum_rows<<<1, 256, 0, d->stream>>>(part, (long)(d->ny - 4) * (d->nz - 4), out);
+  d->kernel_launches += 2;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename T>
+int launch_init_t(lbib_device* d, int what) {
+  using R = typename Pop<T>::R;
+  FluidParamsT<T> p = make_params_t<T>(d, 1);
+  const int block = 256;
+  if (what == 0) {
+    lbib_init_pop<T><<<(unsigned)((d->N + block - 1) / block), block, 0, d->stream>>>(p, (T*)d->f, d->N);
+  } else {
+    const long P = (long)d->ny * d->nz;
+    lbib_init_table<T><<<(unsigned)((P + block - 1) / block), block, 0, d->stream>>>(p, (R*)d->inlet, P);
+    lbib_init_table<T><<<(unsigned)((P + block - 1) / block), block, 0, d->stream>>>(p, (R*)d->outlet, P);
+    d->kernel_launches++;
+  }
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace lbib
+
+#endif

@@ -3,7 +3,8 @@
  * translation units.  Not installed; include/lbib.h is the public ABI.
  *
  * GPU data layout (one fluid grid, several sheets):
- *   f        [19][N] FP64 populations, N = nx*ny*nz, idx = (z*ny + y)*nx + x.
+ *   f        [19][N] populations (FP64; FP32; FP16 or BF16 holding f - w_q),
+ *            N = nx*ny*nz, idx = (z*ny + y)*nx + x.
  *            One buffer, updated in place with the AA access pattern; `parity`
  *            says how the next fused step must read it (0: each cell's own
  *            slots in natural order; 1: the neighbours' opposite slots).
@@ -29,6 +30,15 @@ extern "C" {
 #define LBIB_TILE_CELLS 64
 #define LBIB_CHUNK 32
 
+#ifndef LBIB_PREC_F64
+#define LBIB_PREC_F64 0   /* population storage precisions, as in include/lbib.h */
+#define LBIB_PREC_F32 1
+#define LBIB_PREC_F16 2
+#define LBIB_PREC_BF16 3
+#define LBIB_PREC_SHIFT_FLOW 16
+#endif
+#define LBIB_PREC_TYPE(p) ((p) & 15)
+
 typedef struct lbib_sheet_dev {
   int rows, cols;
   long offset;                   /* first node in the concatenated arrays */
@@ -49,10 +59,12 @@ typedef struct lbib_device {
   double tau, u_l, rho_l, Ks_l, Kb_l, g_l, cs_l;
   int dt;
   double omtau, invtau, kw[3], cs2, cs4, half_dt;
-  /* populations */
-  double* f;
-  double* inlet;
-  double* outlet;
+  /* populations: [19][N] of the storage type of `prec`; inlet/outlet in
+     its arithmetic type (double for FP64, float otherwise) */
+  int prec;
+  void* f;
+  void* inlet;
+  void* outlet;
   int parity;
   long steps;                    /* fused steps since init_df1               */
   int use_bulk;                  /* staged kernel for rows away from walls   */
@@ -103,12 +115,15 @@ typedef struct lbib_device {
 #define LBIB_NSTAGE_TIMED 5      /* forces, spread, fluid, moments, move */
 
 typedef struct lbdev_config {
-  int nx, ny, nz, cube_size, compat;
+  int nx, ny, nz, cube_size, compat, prec;
   double tau, u_l, rho_l, Ks_l, Kb_l, g_l, cs_l;
   int dt;
 } lbdev_config;
 
 int  lbdev_create(lbib_device** out, const lbdev_config* cfg);
+size_t lbdev_pop_bytes(int prec);
+/* The low-precision shift s_q and the (rho, u_x) it carries. */
+void lbdev_shift(const lbib_device* d, float* sh, double* rhos, double* uxs);
 void lbdev_free(lbib_device* d);
 int  lbdev_set_physics(lbib_device* d, const lbdev_config* cfg);
 int  lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_dev* sh, const double* nodes_host);
@@ -121,6 +136,7 @@ int  lbdev_check(lbib_device* d, int* failed_step);  /* syncs, reads error word 
 int  lbdev_get_moments(lbib_device* d, double* rho, double* ux, double* uy, double* uz);
 int  lbdev_get_force(lbib_device* d, double* fx, double* fy, double* fz);
 int  lbdev_get_df1(lbib_device* d, double* out);
+int  lbdev_conservation(lbib_device* d, double* out);
 int  lbdev_get_nodes(lbib_device* d, double* out);
 int  lbdev_set_nodes(lbib_device* d, const double* in);
 int  lbdev_sync(lbib_device* d);

@@ -2,8 +2,9 @@
  * D3Q19 lattice, the AA in-place access rules, and the reference-faithful
  * moment / equilibrium / collision arithmetic shared by the fluid kernels.
  *
- * Compile with -fmad=false: every expression below keeps the operation order
- * of cube_pthread/lbm_ib.c, and contraction into FMA would change roundings.
+ * The FP64 instantiations are compiled with -fmad=false: every expression
+ * below keeps the operation order of cube_pthread/lbm_ib.c, and contraction
+ * into FMA would change roundings.
  *
  * Which cells do what (reference semantics, internal axes, x = flow):
  *   I = [2, nx-3] x [2, ny-3] x [2, nz-3]  cells that collide (lbm_ib.c:1700-1712)
@@ -30,6 +31,8 @@
 #ifndef LBIB_LATTICE_CUH
 #define LBIB_LATTICE_CUH
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -50,12 +53,47 @@ __host__ __device__ constexpr int cz(int q) {
 }
 __host__ __device__ constexpr int opp(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
 
+/* Population storage.  R is the arithmetic type.  FP64 stores f itself.
+ * The low-precision forms store the deviation d_q = f_q - s_q from a fixed
+ * per-direction shift s_q (the rest weights w_q, or the equilibrium of the
+ * inflow state) and do all their arithmetic on deviations in FP32, so the
+ * storage bits and the FP32 mantissa are spent on the part that changes;
+ * s_q == s_opp(q) for the weight shift, and the flow shift keeps the pair
+ * in the parameters, so the AA phase never changes a slot's meaning. */
+template <typename T> struct Pop;
+template <> struct Pop<double> {
+  using R = double;
+  __device__ static __forceinline__ R get(double v) { return v; }
+  __device__ static __forceinline__ double put(R v) { return v; }
+};
+template <> struct Pop<float> {
+  using R = float;
+  __device__ static __forceinline__ R get(float v) { return v; }
+  __device__ static __forceinline__ float put(R v) { return v; }
+};
+template <> struct Pop<__half> {
+  using R = float;
+  __device__ static __forceinline__ R get(__half v) { return __half2float(v); }
+  __device__ static __forceinline__ __half put(R v) { return __float2half_rn(v); }
+};
+template <> struct Pop<__nv_bfloat16> {
+  using R = float;
+  __device__ static __forceinline__ R get(__nv_bfloat16 v) { return __bfloat162float(v); }
+  __device__ static __forceinline__ __nv_bfloat16 put(R v) { return __float2bfloat16_rn(v); }
+};
+
 enum CellKind { K_FAST = 0, K_WALL = 1, K_SEMI = 2, K_TABLE = 3 };
 
-struct FluidParams {
-  double* f;
-  const double* inlet;
-  const double* outlet;
+/* Everything a fluid kernel needs.  inlet/outlet hold populations in the
+ * arithmetic type and in the stored representation (f for FP64, f - s_q
+ * otherwise).  sh, rhos, uxs: the low-precision shift s_q and the density
+ * and x velocity it carries (sum_q s_q, sum_q c_qx s_q / sum_q s_q). */
+template <typename T>
+struct FluidParamsT {
+  using R = typename Pop<T>::R;
+  T* f;
+  const R* inlet;
+  const R* outlet;
   long N;
   int nx, ny, nz;
   int zin_hi, yskip_z0, first;
@@ -66,9 +104,30 @@ struct FluidParams {
   const int* slot_prev;  /* (rho, u)(t-1) tiles */
   const double* Uprev;
   int ntx, nty;
+  float sh[19];
+  double rhos, uxs;
 };
 
-__device__ __forceinline__ int classify(const FluidParams& p, int x, int y, int z) {
+/* A bounce-back link delivers this cell's own outgoing population opp(q) as
+ * the incoming q; as a deviation it moves from s_opp(q) to s_q.  Before the
+ * first step the slot still holds the initial population q itself. */
+template <typename T>
+__device__ __forceinline__ typename Pop<T>::R bounced(const FluidParamsT<T>& p, int q, typename Pop<T>::R v) {
+  if constexpr (sizeof(T) == 8) return v;
+  else return p.first ? v : v + (p.sh[opp(q)] - p.sh[q]);
+}
+
+/* The stored value of a population the reference holds as 0 (its calloc'd
+ * df2 where nothing writes): 0, or -s_q as a deviation. */
+template <typename T>
+__device__ __forceinline__ typename Pop<T>::R zero_pop(const FluidParamsT<T>& p, int q) {
+  if constexpr (sizeof(T) == 8) return 0.0;
+  else return -p.sh[q];
+}
+using FluidParams = FluidParamsT<double>;
+
+template <typename P>
+__device__ __forceinline__ int classify(const P& p, int x, int y, int z) {
   if (x == 2 || x == p.nx - 3) return (z <= p.zin_hi) ? K_TABLE : K_SEMI;
   if (y == 2 || y == p.ny - 3 || z == 2 || z == p.nz - 3) return K_WALL;
   return K_FAST;
@@ -79,13 +138,14 @@ __device__ __forceinline__ long link_offset(int q, long sy, long sz) {
 }
 
 /* Pre-collision populations of cell (x, y, z) in I for a step of parity PAR. */
-template <int PAR>
-__device__ __forceinline__ void load_pre(const FluidParams& p, int x, int y, int z, long idx, int kind,
-                                         double f[19]) {
+template <int PAR, typename T>
+__device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y, int z, long idx, int kind,
+                                         typename Pop<T>::R f[19]) {
+  using R = typename Pop<T>::R;
   const long N = p.N;
-  const double* __restrict__ F = p.f;
+  const T* __restrict__ F = p.f;
   if (kind == K_TABLE) {
-    const double* t = (x == 2) ? p.inlet : p.outlet;
+    const R* t = (x == 2) ? p.inlet : p.outlet;
     const long P = (long)p.ny * p.nz;
     const long pi = (long)y * p.nz + z;
 #pragma unroll
@@ -96,8 +156,8 @@ __device__ __forceinline__ void load_pre(const FluidParams& p, int x, int y, int
   if (kind == K_FAST) {
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
-      if (PAR == 0) f[q] = F[q * N + idx];
-      else f[q] = F[opp(q) * N + idx - link_offset(q, sy, sz)];
+      if (PAR == 0) f[q] = Pop<T>::get(F[q * N + idx]);
+      else f[q] = Pop<T>::get(F[opp(q) * N + idx - link_offset(q, sy, sz)]);
     }
     return;
   }
@@ -109,56 +169,57 @@ __device__ __forceinline__ void load_pre(const FluidParams& p, int x, int y, int
     const bool zin = zs >= 2 && zs <= p.nz - 3;
     const bool xin = xs >= 2 && xs <= p.nx - 3;
     if (xin && yin && zin) {
-      if (PAR == 0) f[q] = F[q * N + idx];
-      else f[q] = F[opp(q) * N + idx - link_offset(q, sy, sz)];
+      if (PAR == 0) f[q] = Pop<T>::get(F[q * N + idx]);
+      else f[q] = Pop<T>::get(F[opp(q) * N + idx - link_offset(q, sy, sz)]);
     } else {
       const bool zero = !p.first && (kind == K_SEMI || (yskip && !yin && zin));
-      f[q] = zero ? 0.0 : F[q * N + idx];
+      f[q] = zero ? zero_pop(p, q) : bounced(p, q, Pop<T>::get(F[q * N + idx]));
     }
   }
 }
 
 /* Post-collision populations of cell (x, y, z) in I for a step of parity PAR. */
-template <int PAR>
-__device__ __forceinline__ void store_post(const FluidParams& p, int x, int y, int z, long idx, int kind,
-                                           const double f[19]) {
+template <int PAR, typename T>
+__device__ __forceinline__ void store_post(const FluidParamsT<T>& p, int x, int y, int z, long idx, int kind,
+                                           const typename Pop<T>::R f[19]) {
   const long N = p.N;
-  double* __restrict__ F = p.f;
+  T* __restrict__ F = p.f;
   if (PAR == 0) {
 #pragma unroll
-    for (int q = 0; q < 19; ++q) F[opp(q) * N + idx] = f[q];
+    for (int q = 0; q < 19; ++q) F[opp(q) * N + idx] = Pop<T>::put(f[q]);
     return;
   }
   const long sy = p.nx, sz = (long)p.nx * p.ny;
   if (kind == K_FAST) {
 #pragma unroll
-    for (int q = 0; q < 19; ++q) F[q * N + idx + link_offset(q, sy, sz)] = f[q];
+    for (int q = 0; q < 19; ++q) F[q * N + idx + link_offset(q, sy, sz)] = Pop<T>::put(f[q]);
     return;
   }
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
     const int xt = x + cx(q), yt = y + cy(q), zt = z + cz(q);
     const bool in = xt >= 2 && xt <= p.nx - 3 && yt >= 2 && yt <= p.ny - 3 && zt >= 2 && zt <= p.nz - 3;
-    if (in) F[q * N + idx + link_offset(q, sy, sz)] = f[q];
-    else F[opp(q) * N + idx] = f[q];
+    if (in) F[q * N + idx + link_offset(q, sy, sz)] = Pop<T>::put(f[q]);
+    else F[opp(q) * N + idx] = Pop<T>::put(f[q]);
   }
 }
 
 /* compute_rho_and_u, cube_pthread/lbm_ib.c:2493-2528: sums in q order.
  * Terms with c = 0 are dropped from the momentum sums: for finite values
  * s + 0*f == s, so the result is the same number. */
-__device__ __forceinline__ void moments(const double f[19], double Fx, double Fy, double Fz, double half_dt,
-                                        double g, double& rho, double& ux, double& uy, double& uz) {
-  double s1 = f[0];
+template <typename R>
+__device__ __forceinline__ void moments(const R f[19], R Fx, R Fy, R Fz, R half_dt, R g, R& rho, R& ux, R& uy,
+                                        R& uz) {
+  R s1 = f[0];
 #pragma unroll
   for (int q = 1; q < 19; ++q) s1 = s1 + f[q];
-  double s2 = 0.0 * f[0];
+  R s2 = R(0) * f[0];
   s2 = s2 + f[1]; s2 = s2 - f[2]; s2 = s2 + f[7]; s2 = s2 - f[8]; s2 = s2 + f[9];
   s2 = s2 - f[10]; s2 = s2 + f[15]; s2 = s2 - f[16]; s2 = s2 + f[17]; s2 = s2 - f[18];
-  double s3 = 0.0 * f[0];
+  R s3 = R(0) * f[0];
   s3 = s3 - f[5]; s3 = s3 + f[6]; s3 = s3 - f[11]; s3 = s3 + f[12]; s3 = s3 + f[13];
   s3 = s3 - f[14]; s3 = s3 - f[15]; s3 = s3 + f[16]; s3 = s3 + f[17]; s3 = s3 - f[18];
-  double s4 = 0.0 * f[0];
+  R s4 = R(0) * f[0];
   s4 = s4 + f[3]; s4 = s4 - f[4]; s4 = s4 + f[7]; s4 = s4 - f[8]; s4 = s4 - f[9];
   s4 = s4 + f[10]; s4 = s4 + f[11]; s4 = s4 - f[12]; s4 = s4 + f[13]; s4 = s4 - f[14];
   rho = s1;
@@ -169,8 +230,9 @@ __device__ __forceinline__ void moments(const double f[19], double Fx, double Fy
 
 /* c . u for each direction, as (c0*ux + c1*uy) + c2*uz evaluates with
  * c in {0, +-1}; opposite directions give exact negatives. */
-__device__ __forceinline__ void velocity_dots(double ux, double uy, double uz, double cu[19]) {
-  cu[0] = 0.0;
+template <typename R>
+__device__ __forceinline__ void velocity_dots(R ux, R uy, R uz, R cu[19]) {
+  cu[0] = R(0);
   cu[1] = ux;        cu[2] = -ux;
   cu[3] = uz;        cu[4] = -uz;
   cu[5] = -uy;       cu[6] = uy;
@@ -187,31 +249,32 @@ __device__ __forceinline__ void velocity_dots(double ux, double uy, double uz, d
  * written there (true divisions by cs^2 and cs^4); without one that term is
  * +-0 in the reference and is skipped. */
 /* Guo forcing term of direction q as lbm_ib.c:1740-1754 writes it. */
-__device__ __forceinline__ double guo(int q, double ux, double uy, double uz, double Fx, double Fy, double Fzg,
-                                      const FluidParams& p) {
-  const double c0 = (double)cx(q), c1 = (double)cy(q), c2 = (double)cz(q);
-  const double kw = (q == 0) ? p.kw0 : ((q <= 6) ? p.kw1 : p.kw2);
-  const double A = (c0 - ux) * Fx + (c1 - uy) * Fy + (c2 - uz) * Fzg;
-  const double B = c0 * ux + c1 * uy + c2 * uz;
-  const double C = c0 * Fx + c1 * Fy + c2 * Fzg;
-  return kw * (A / p.cs2 + B / p.cs4 * C);
+template <typename R, typename P>
+__device__ __forceinline__ R guo(int q, R ux, R uy, R uz, R Fx, R Fy, R Fzg, const P& p) {
+  const R c0 = (R)cx(q), c1 = (R)cy(q), c2 = (R)cz(q);
+  const R kw = (R)((q == 0) ? p.kw0 : ((q <= 6) ? p.kw1 : p.kw2));
+  const R A = (c0 - ux) * Fx + (c1 - uy) * Fy + (c2 - uz) * Fzg;
+  const R B = c0 * ux + c1 * uy + c2 * uz;
+  const R C = c0 * Fx + c1 * Fy + c2 * Fzg;
+  return kw * (A / (R)p.cs2 + B / (R)p.cs4 * C);
 }
 
+template <typename R>
 struct Relax {
-  double ux, uy, uz, Fx, Fy, Fzg, t6, om, it;
+  R ux, uy, uz, Fx, Fy, Fzg, t6, om, it;
 };
 
 /* One opposite pair (qa, qb) with c_qa . u = cu: both equilibria share
  * 3cu, cu^2 and 1.5 u^2, and 1 + (-3cu) == 1 - 3cu exactly.  With a force
  * the Guo term is added after the relaxation, as the reference sums it. */
-template <bool FORCED, int QA, int QB>
-__device__ __forceinline__ void relax_pair(double* f, double cu, double wr, const Relax& r, const FluidParams& p) {
-  const double a3 = 3.0 * cu;
-  const double sq = 4.5 * (cu * cu);
-  const double ea = wr * (1.0 + a3 + sq - r.t6);
-  const double eb = wr * (1.0 + (-a3) + sq - r.t6);
-  double va = f[QA] * r.om + r.it * ea;
-  double vb = f[QB] * r.om + r.it * eb;
+template <bool FORCED, int QA, int QB, typename R, typename P>
+__device__ __forceinline__ void relax_pair(R* f, R cu, R wr, const Relax<R>& r, const P& p) {
+  const R a3 = R(3.0) * cu;
+  const R sq = R(4.5) * (cu * cu);
+  const R ea = wr * (R(1.0) + a3 + sq - r.t6);
+  const R eb = wr * (R(1.0) + (-a3) + sq - r.t6);
+  R va = f[QA] * r.om + r.it * ea;
+  R vb = f[QB] * r.om + r.it * eb;
   if (FORCED) {
     va = va + guo(QA, r.ux, r.uy, r.uz, r.Fx, r.Fy, r.Fzg, p);
     vb = vb + guo(QB, r.ux, r.uy, r.uz, r.Fx, r.Fy, r.Fzg, p);
@@ -220,18 +283,17 @@ __device__ __forceinline__ void relax_pair(double* f, double cu, double wr, cons
   f[QB] = vb;
 }
 
-template <bool FORCED>
-__device__ __forceinline__ void collide(double f[19], double rho, double ux, double uy, double uz,
-                                        double Fx, double Fy, double Fz, const FluidParams& p) {
-  Relax r;
+template <bool FORCED, typename R, typename P>
+__device__ __forceinline__ void collide(R f[19], R rho, R ux, R uy, R uz, R Fx, R Fy, R Fz, const P& p) {
+  Relax<R> r;
   r.ux = ux; r.uy = uy; r.uz = uz;
-  r.Fx = Fx; r.Fy = Fy; r.Fzg = FORCED ? Fz + rho * p.g : 0.0;
-  r.t6 = 1.5 * (ux * ux + uy * uy + uz * uz);
-  r.om = p.omtau; r.it = p.invtau;
-  const double wr0 = 1.0 / 3.0 * rho;
-  const double wr1 = 1.0 / 18.0 * rho;
-  const double wr2 = 1.0 / 36.0 * rho;
-  double v0 = f[0] * r.om + r.it * (wr0 * (1.0 - r.t6));
+  r.Fx = Fx; r.Fy = Fy; r.Fzg = FORCED ? Fz + rho * (R)p.g : R(0);
+  r.t6 = R(1.5) * (ux * ux + uy * uy + uz * uz);
+  r.om = (R)p.omtau; r.it = (R)p.invtau;
+  const R wr0 = R(1.0 / 3.0) * rho;
+  const R wr1 = R(1.0 / 18.0) * rho;
+  const R wr2 = R(1.0 / 36.0) * rho;
+  R v0 = f[0] * r.om + r.it * (wr0 * (R(1.0) - r.t6));
   if (FORCED) v0 = v0 + guo(0, ux, uy, uz, Fx, Fy, r.Fzg, p);
   f[0] = v0;
   relax_pair<FORCED, 1, 2>(f, ux, wr1, r, p);

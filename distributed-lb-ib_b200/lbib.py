@@ -23,6 +23,13 @@ COMPAT_YWALL_CUBES_X = 2
 COMPAT_INOUT_PTHREAD = 4
 COMPAT_ALL = 7
 
+PREC_F64, PREC_F32, PREC_F16, PREC_BF16, PREC_SHIFT_FLOW = 0, 1, 2, 3, 16
+# population storage: FP64 (the drop-in), or deviations from the rest
+# weights ("f32", "f16", "bf16") or from the inflow equilibrium ("...-flow")
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16, "bf16": PREC_BF16,
+              "f32-flow": PREC_F32 | PREC_SHIFT_FLOW, "f16-flow": PREC_F16 | PREC_SHIFT_FLOW,
+              "bf16-flow": PREC_BF16 | PREC_SHIFT_FLOW}
+
 DUMP_NONE = 0
 DUMP_FIELDVIEW = 1
 DUMP_BINARY = 2
@@ -43,6 +50,7 @@ EXPORTED = [
     "lbib_free", "lbib_get_moments", "lbib_get_force", "lbib_get_df1", "lbib_get_sheet", "lbib_set_sheet",
     "lbib_run", "lbib_synchronize", "lbib_stream", "lbib_case_create", "lbib_case_free", "lbib_stage",
     "lbib_device_count", "lbib_kernel_launches", "lbib_profile_begin", "lbib_profile_end",
+    "lbib_set_precision", "lbib_case_create_prec", "lbib_spread_force_noalloc", "lbib_conservation_sums",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -74,6 +82,9 @@ def load() -> C.CDLL:
     lib = C.CDLL(LIB_PATH)
     lib.lbib_case_create.restype = C.c_void_p
     lib.lbib_case_create.argtypes = [C.c_int] * 5 + [_ip, _ip] + [_dp] * 5 + [C.c_double] * 4 + [C.c_int]
+    lib.lbib_case_create_prec.restype = C.c_void_p
+    lib.lbib_case_create_prec.argtypes = lib.lbib_case_create.argtypes + [C.c_int]
+    lib.lbib_set_precision.argtypes = [C.c_void_p, C.c_int]
     lib.lbib_case_free.argtypes = [C.c_void_p]
     lib.lbib_case_free.restype = None
     lib.lbib_run.argtypes = [C.c_void_p, C.c_int]
@@ -82,6 +93,7 @@ def load() -> C.CDLL:
         getattr(lib, n).argtypes = [C.c_void_p] + [_dp] * 4
     lib.lbib_get_force.argtypes = [C.c_void_p] + [_dp] * 3
     lib.lbib_get_df1.argtypes = [C.c_void_p, _dp]
+    lib.lbib_conservation_sums.argtypes = [C.c_void_p, _dp]
     lib.lbib_get_sheet.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.lbib_set_sheet.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.lbib_synchronize.argtypes = [C.c_void_p]
@@ -130,9 +142,11 @@ class Solver:
     ``case`` is any object with ``nx, ny, nz, cube_size, tau, u_l, Ks_l, Kb_l,
     compat`` and ``sheets`` (each with ``rows, cols, width, height, x0, y0,
     z0``), in the reference's internal axes (x = flow direction).
+    ``precision`` (a key of PRECISIONS) selects the population storage;
+    "f64" is the drop-in path.
     """
 
-    def __init__(self, case):
+    def __init__(self, case, precision: str = "f64"):
         lib = load()
         self.lib = lib
         self.case = case
@@ -141,12 +155,15 @@ class Solver:
         ia = lambda v: (C.c_int * k)(*v)
         da = lambda v: (C.c_double * k)(*v)
         lib.lbib_clear_error()
-        self.gv = lib.lbib_case_create(
+        if precision not in PRECISIONS:
+            raise LbibError(f"unknown precision {precision!r}")
+        self.precision = precision
+        self.gv = lib.lbib_case_create_prec(
             case.nx, case.ny, case.nz, case.cube_size, k,
             ia([s.rows for s in sh]), ia([s.cols for s in sh]),
             da([s.width for s in sh]), da([s.height for s in sh]),
             da([s.x0 for s in sh]), da([s.y0 for s in sh]), da([s.z0 for s in sh]),
-            case.tau, case.u_l, case.Ks_l, case.Kb_l, case.compat)
+            case.tau, case.u_l, case.Ks_l, case.Kb_l, case.compat, PRECISIONS[precision])
         if not self.gv:
             rc = lib.lbib_last_error()
             lib.lbib_clear_error()
@@ -211,6 +228,12 @@ class Solver:
         a = np.empty(19 * self.N)
         _check(self.lib.lbib_get_df1(self.gv, _ptr(a)), "lbib_get_df1")
         return a.reshape(19, c.nz, c.ny, c.nx)
+
+    def conservation(self) -> np.ndarray:
+        """[mass, x, y, z momentum] of the populations, FP64 fixed-order sums."""
+        a = np.empty(4)
+        _check(self.lib.lbib_conservation_sums(self.gv, _ptr(a)), "lbib_conservation_sums")
+        return a
 
     def sheet(self, k: int = 0) -> np.ndarray:
         s = self.case.sheets[k]

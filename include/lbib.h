@@ -136,6 +136,7 @@ typedef struct gv_t {
   struct lbib_device* dev;         /* NULL until gen_fluid_grid          */
   int lbib_compat;                 /* LBIB_COMPAT_* bits, see below      */
   int lbib_dump_mode;              /* LBIB_DUMP_* bits for do_thread     */
+  int lbib_precision;              /* LBIB_PREC_* population storage     */
 }* GV;
 
 /* mpi/do_thread.h:242-245 */
@@ -150,6 +151,21 @@ typedef struct lv_t {
 #define LBIB_COMPAT_YWALL_CUBES_X 2  /* y-wall z range clipped with num_cubes_x, lbm_ib.c:2378,2414 */
 #define LBIB_COMPAT_INOUT_PTHREAD 4  /* inlet/outlet copy loops BK < num_cubes_x, lbm_ib.c:2800-2882 */
 #define LBIB_COMPAT_ALL           7
+
+/* Population storage of the fluid step (no reference counterpart; the
+ * reference stores FP64).  LBIB_PREC_F64 is the drop-in: results equal the
+ * reference's to rounding.  The others trade accuracy for HBM traffic: they
+ * store the deviation f_q - s_q from a fixed shift in FP32, FP16 or BF16
+ * and do moments, equilibrium and collision on deviations in FP32 (FMA
+ * contraction allowed).  The shift is the rest weights w_q, or, with
+ * LBIB_PREC_SHIFT_FLOW or'ed in, the equilibrium of the initial state
+ * (rho_l, u_l, 0, 0).  Forces, the moments handed to the sheets and the
+ * sheets stay FP64. */
+#define LBIB_PREC_F64        0
+#define LBIB_PREC_F32        1
+#define LBIB_PREC_F16        2
+#define LBIB_PREC_BF16       3
+#define LBIB_PREC_SHIFT_FLOW 16
 
 /* What do_thread writes at time == 1 and every gv->dump steps. */
 #define LBIB_DUMP_NONE      0
@@ -246,6 +262,12 @@ void save_fiber_sub_grid_cord_ef_use_fv(GV gv, int start_y, int start_z, int end
  * it also resets the initial velocity to (u_l, 0, 0). */
 int lbib_set_params(GV gv, double tau, double u_l, double Ks_l, double Kb_l);
 int lbib_set_compat(GV gv, int flags);
+/* Selects the population storage (LBIB_PREC_*); init_gv_constant sets F64.
+ * Call before init_gv: when the grid's GPU state exists it is rebuilt in
+ * the new precision (populations zeroed; run init_eqlbrmdistrfuncDF0,
+ * init_df1 and init_df_inout after).  LBIB_E_STATE once sheets are
+ * uploaded, LBIB_E_ARG for an unknown value. */
+int lbib_set_precision(GV gv, int precision);
 int lbib_last_error(void);
 const char* lbib_error_string(int code);
 void lbib_clear_error(void);
@@ -261,6 +283,10 @@ void lbib_free(GV gv);
 int lbib_get_moments(GV gv, double* rho, double* ux, double* uy, double* uz);
 int lbib_get_force(GV gv, double* fx, double* fy, double* fz);
 int lbib_get_df1(GV gv, double* out);            /* [19][N], cells of [2,n-3]^3 */
+/* out[4] = mass and x, y, z momentum of the populations of [2,n-3]^3 as
+ * the next step reads them, summed in FP64 in a fixed order (the same
+ * value on every run). */
+int lbib_conservation_sums(GV gv, double* out);
 int lbib_get_sheet(GV gv, int sheet, double* out);
 int lbib_set_sheet(GV gv, int sheet, const double* in);
 int lbib_run(GV gv, int nsteps);                 /* do_thread for nsteps steps */
@@ -284,6 +310,13 @@ GV lbib_case_create(int nx, int ny, int nz, int cube_size, int nsheets,
                     const double* width, const double* height,
                     const double* x0, const double* y0, const double* z0,
                     double tau, double u_l, double Ks_l, double Kb_l, int compat);
+/* lbib_case_create with a population storage precision (LBIB_PREC_*). */
+GV lbib_case_create_prec(int nx, int ny, int nz, int cube_size, int nsheets,
+                         const int* rows, const int* cols,
+                         const double* width, const double* height,
+                         const double* x0, const double* y0, const double* z0,
+                         double tau, double u_l, double Ks_l, double Kb_l, int compat,
+                         int precision);
 void lbib_case_free(GV gv);
 /* Calls one stage by number, in do_thread order: 0 bending, 1 stretching,
  * 2 elastic, 3 spread (fiber_SpreadForce + fluid_get_SpreadForce),

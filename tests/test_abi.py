@@ -79,3 +79,22 @@ def test_drop_in_host_setup_matches_oracle(lbib_built, oracle_built, tmp_path):
     # gen_fiber_sheet positions (before init_gv's shift) equal the oracle's minus u_l*dt
     o = P.Oracle(P.Case(24, 12, 12, case.sheets, u_l=0.0))
     np.testing.assert_array_equal(nodes, o.sheet()[..., :3].reshape(-1, 3))
+
+
+def test_precision_arguments_checked_before_any_gpu_call(lbib_built):
+    """Unknown storage precisions are refused on the host (no CUDA call)."""
+    lib = lbib.load()
+    one_i = (ctypes.c_int * 1)(4)
+    one_d = (ctypes.c_double * 1)(1.0)
+    lib.lbib_clear_error()
+    for bad in (-1, 4, 16, 20, 99):
+        gv = lib.lbib_case_create_prec(32, 16, 16, 4, 1, one_i, one_i, one_d, one_d, one_d, one_d, one_d,
+                                       0.6, 0.01, 0.05, 0.005, P.COMPAT_ALL, bad)
+        assert not gv
+        assert lib.lbib_last_error() == -1
+        lib.lbib_clear_error()
+    assert lib.lbib_set_precision(None, lbib.PREC_F16) == -1
+    lib.lbib_clear_error()
+    assert lbib.PRECISIONS["f64"] == 0 and lbib.PRECISIONS["f16-flow"] == 18
+    with pytest.raises(lbib.LbibError):
+        lbib.Solver(small_case(), precision="f8")

@@ -1,0 +1,108 @@
+"""Low-precision population storage against the FP64 drop-in.
+
+The FP64 path is pinned to the oracle bit for bit (test_gpu_parity.py); the
+FP32 / FP16 / BF16 forms store deviations from a shift and do FP32
+arithmetic, so they are judged by their error against the FP64 solution of
+the same case.  Bars (relative L2 of u over the fluid interior, tip =
+mean x-displacement of the last fiber row, mass = FP64 population sum):
+
+  form        velocity   tip      |mass - mass64| / mass64
+  f32         1e-4       1e-4     1e-7
+  f16-flow    1e-3       2e-3     1e-5
+  f16         1e-2       5e-3     1e-5
+  bf16-flow   2e-2       2e-2     1e-4
+  bf16        5e-2       2e-2     2e-4
+
+on the 128x64x64 lattice with one 52x52 sheet after 1000 steps, and the
+starting state to the storage rounding.  The FP64 sums are also checked
+against the oracle's populations.
+"""
+import numpy as np
+import pytest
+
+import lbib
+import precision
+import pyoracle as P
+from cases import c0_case, small_case
+
+pytestmark = pytest.mark.gpu
+
+LP = ["f32", "f16", "bf16", "f32-flow", "f16-flow", "bf16-flow"]
+# lattice velocities in the library's q order (the reference's c table,
+# cube_pthread/lbm_ib.c:777-833, in internal axes)
+C = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 0, 1], [0, 0, -1], [0, -1, 0], [0, 1, 0],
+              [1, 0, 1], [-1, 0, -1], [1, 0, -1], [-1, 0, 1], [0, -1, 1], [0, 1, -1],
+              [0, 1, 1], [0, -1, -1], [1, -1, 0], [-1, 1, 0], [1, 1, 0], [-1, -1, 0]], dtype=np.float64)
+BARS = {
+    "f32": (1e-4, 1e-4, 1e-7),
+    "f16-flow": (1e-3, 2e-3, 1e-5),
+    "f16": (1e-2, 5e-3, 1e-5),
+    "bf16-flow": (2e-2, 2e-2, 1e-4),
+    "bf16": (5e-2, 2e-2, 2e-4),
+}
+# largest |f - f64| of the initial populations: half an ulp of the stored deviation
+INIT_TOL = {"f32": 1e-9, "f32-flow": 1e-9, "f16": 2e-6, "f16-flow": 1e-8, "bf16": 2e-5, "bf16-flow": 1e-7}
+
+
+def interior(case):
+    return (slice(None), slice(2, case.nz - 2), slice(2, case.ny - 2), slice(2, case.nx - 2))
+
+
+@pytest.mark.parametrize("prec", LP)
+def test_initial_populations_match_f64(gpu, prec):
+    case = small_case(32, 16, 16, 8, 8, 10.0)
+    with lbib.Solver(case, "f64") as s:
+        ref = s.df1()[interior(case)]
+    with lbib.Solver(case, prec) as s:
+        got = s.df1()[interior(case)]
+    assert np.max(np.abs(got - ref)) <= INIT_TOL[prec]
+
+
+def test_f64_conservation_sums_match_oracle(gpu, oracle_built):
+    case = small_case(24, 12, 12, 6, 6, 8.0)
+    o = P.Oracle(case, cr_cos=True)
+    o.run(12)
+    with lbib.Solver(case) as s:
+        s.run(12)
+        got = s.conservation()
+        again = s.conservation()
+    df = o.df(0)[interior(case)]
+    want = [df.sum()] + [np.tensordot(C[:, k], df, 1).sum() for k in range(3)]
+    np.testing.assert_array_equal(got, again)  # fixed summation order
+    assert abs(got[0] - want[0]) <= 1e-13 * abs(want[0])
+    np.testing.assert_allclose(got[1:], want[1:], rtol=0, atol=1e-12 * abs(want[0]))
+
+
+@pytest.mark.parametrize("prec", LP)
+def test_low_precision_sums_match_populations(gpu, prec):
+    case = small_case(32, 16, 16, 8, 8, 10.0)
+    with lbib.Solver(case, prec) as s:
+        s.run(7)
+        got = s.conservation()
+        df = s.df1()[interior(case)]
+    assert abs(got[0] - df.sum()) <= 1e-12 * df.sum()
+
+
+@pytest.fixture(scope="module")
+def c0_reference(gpu):
+    return precision.run_case(c0_case(), 1000, "f64")
+
+
+@pytest.mark.parametrize("prec", sorted(BARS))
+def test_error_against_f64_after_1000_steps(c0_reference, prec):
+    case = c0_case()
+    r = precision.compare(c0_reference, precision.run_case(case, 1000, prec), case)
+    v, tip, mass = BARS[prec]
+    assert r["velocity_rel_l2"] <= v, r
+    assert r["tip_displacement_rel"] <= tip, r
+    assert abs(r["mass_vs_f64"]) <= mass, r
+
+
+def test_precision_switch_rebuilds_state(gpu):
+    """lbib_set_precision before init_gv rebuilds the GPU state; after it, refused."""
+    lib = lbib.load()
+    case = small_case(32, 16, 16, 8, 8, 10.0)
+    with lbib.Solver(case, "f16-flow") as s:
+        lib.lbib_clear_error()
+        assert lib.lbib_set_precision(s.gv, lbib.PREC_F32) == -4  # sheets already uploaded
+        lib.lbib_clear_error()
