@@ -302,7 +302,13 @@ def run_lbib(args):
     import torch
     torch.cuda.set_device(local)
     case = make_case(args.config)
-    solver = lbib.Solver(case)
+    solver = lbib.Solver(case, precision=args.precision)
+    tuned = None
+    if args.variant is not None:
+        solver.set_variant(args.variant)
+    elif solver.variants() > 1:
+        best, ms_v = solver.autotune(8)
+        tuned = {"variant": best, "ms_per_step": ms_v}
     init_sheet = np.ascontiguousarray(solver.sheet(0))   # the host copy a user starts from
     stream = torch.cuda.ExternalStream(solver.stream)
     solver.run(args.warmup)
@@ -329,7 +335,8 @@ def run_lbib(args):
     value = whole_job_mlups(case.ncells, args.steps, world, ms_max / 1e3)
 
     fluid_cells = (case.nx - 4) * (case.ny - 4) * (case.nz - 4)
-    bytes_launch = fluid_cells * BYTES_PER_UPDATE
+    pop_bytes = {"f64": 8, "f32": 4}.get(args.precision.split("-")[0], 2)
+    bytes_launch = fluid_cells * 19 * 2 * pop_bytes
     fluid_ms = stage_ms["fluid"] / max(nprof, 1)
     achieved = bytes_launch / (fluid_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
@@ -377,7 +384,7 @@ def run_lbib(args):
                              "kernel": "lbib_fluid_step (fused D3Q19 AA step)",
                              "bytes_per_launch": bytes_launch, "launch_ms": fluid_ms},
                 "stages_ms_per_step": {k: v / max(nprof, 1) for k, v in stage_ms.items()},
-                "gpu_launches": launches,
+                "gpu_launches": launches, "autotune": tuned,
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)
     group.close()
@@ -394,6 +401,10 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="fluid-kernel variant (default: autotuned when there are several)")
+    ap.add_argument("--precision", default="f64",
+                    help="population storage of the timed leg: f64 (the drop-in), f32, f16, bf16, *-flow")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

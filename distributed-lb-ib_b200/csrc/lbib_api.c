@@ -265,6 +265,23 @@ int lbib_set_precision(GV gv, int precision) {
   return LBIB_OK;
 }
 
+int lbib_kernel_variants(GV gv) {
+  if (!gv || !gv->dev) return set_error(LBIB_E_STATE);
+  return lbdev_variants(gv->dev);
+}
+
+int lbib_set_kernel_variant(GV gv, int variant) {
+  if (!gv || !gv->dev) return set_error(LBIB_E_STATE);
+  return lbdev_set_variant(gv->dev, variant) ? set_error(LBIB_E_ARG) : LBIB_OK;
+}
+
+int lbib_autotune(GV gv, int steps, double* ms_per_variant, int max_variants) {
+  if (!gv || !gv->dev) return set_error(LBIB_E_STATE);
+  int best = 0;
+  int rc = lbdev_autotune(gv->dev, steps, ms_per_variant, max_variants, &best);
+  return rc ? set_error(rc) : best;
+}
+
 /* ---- the step -------------------------------------------------------- */
 
 static int stage(LV lv, int which) {

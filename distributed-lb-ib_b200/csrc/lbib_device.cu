@@ -19,6 +19,7 @@ int lbdev_launch_field_moments(lbib_device* d, double* rho, double* ux, double* 
 int lbdev_launch_gather_df1(lbib_device* d, double* out);
 int lbdev_launch_init(lbib_device* d, int what);
 int lbdev_launch_sums(lbib_device* d, double* part, double* out);
+int lbdev_lp_variants(int prec);
 int lbdev_launch_fiber_forces(lbib_device* d, int k);
 int lbdev_launch_spread(lbib_device* d, int step);
 int lbdev_launch_move(lbib_device* d);
@@ -118,13 +119,16 @@ extern "C" void lbdev_shift(const lbib_device* d, float* sh, double* rhos, doubl
 }
 
 /* Rows (y, z) of I that the generic fused kernel processes: all of them, or,
- * with the staged kernel on, those it does not take (next to the walls, or
- * above zin_hi).  The staged kernel needs even nx for aligned copies. */
+ * with the bulk kernels on, those they do not take (next to the walls, or
+ * above zin_hi).  The bulk kernels need nx divisible by the cells they move
+ * per aligned access. */
 static int build_rows(lbib_device* d) {
   const char* env = getenv("LBIB_FLUID_BULK");
   int ry = 0, rz = 0;
-  d->use_bulk = !(env && env[0] == '0') && LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 && (d->nx % 2 == 0) &&
-                lbdev_bulk_rows(d, &ry, &rz);
+  /* cells per aligned 8-byte word of the low-precision bulk kernel; the
+     FP64 two-cell kernel wants even nx */
+  const int v = LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 ? 2 : (int)(8 / lbdev_pop_bytes(d->prec));
+  d->use_bulk = !(env && env[0] == '0') && (d->nx % v == 0) && lbdev_bulk_rows(d, &ry, &rz);
   const int zb = 2 + rz;  /* last z row of the staged kernel */
   long cap = (long)(d->ny - 4) * (d->nz - 4);
   int* h = (int*)malloc(sizeof(int) * 2 * cap);
@@ -184,8 +188,50 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   if (!rc) rc = build_rows(d);
   if (rc) { lbdev_free(d); return rc; }
   d->cur = 0;
+  d->lp_variant = -1;
   *out = d;
   return 0;
+}
+
+extern "C" int lbdev_variants(const lbib_device* d) { return lbdev_lp_variants(d->prec); }
+
+extern "C" int lbdev_set_variant(lbib_device* d, int v) {
+  if (v < -1 || v >= lbdev_variants(d)) return -1;
+  d->lp_variant = v;
+  return 0;
+}
+
+extern "C" int lbdev_autotune(lbib_device* d, int steps, double* ms, int max_ms, int* best) {
+  if (!d->have_df1 || !d->have_inout || !d->tile_slot[0]) return -4;
+  if (d->steps != 0) return -4;
+  if (steps < 2) steps = 2;
+  steps += steps & 1;                      /* whole even/odd pairs */
+  const int n = lbdev_variants(d);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int rc = 0, pick = 0;
+  float best_ms = 0.0f;
+  for (int v = 0; v < n && !rc; ++v) {
+    d->lp_variant = v;
+    for (int k = 0; k < 2 && !rc; ++k) rc = lbdev_launch_fluid_step(d);   /* warm-up */
+    if (!rc && cudaEventRecord(e0, d->stream) != cudaSuccess) rc = -2;
+    for (int k = 0; k < steps && !rc; ++k) rc = lbdev_launch_fluid_step(d);
+    if (!rc && cudaEventRecord(e1, d->stream) != cudaSuccess) rc = -2;
+    float t = 0.0f;
+    if (!rc && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)) rc = -2;
+    if (!rc) {
+      if (ms && v < max_ms) ms[v] = t / steps;
+      if (v == 0 || t < best_ms) { best_ms = t; pick = v; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  d->lp_variant = pick;
+  if (best) *best = pick;
+  /* the trials stepped the fluid; start again from the initial state */
+  const int rc2 = lbdev_init_df1(d);
+  return rc ? rc : rc2;
 }
 
 extern "C" void lbdev_free(lbib_device* d) {

@@ -49,25 +49,39 @@ struct Mom {
   R rho, ux, uy, uz;
 };
 
-/* Deviation-form BGK + Guo for one opposite pair (qa, qb), c_qa = -c_qb:
- *   a = c.u, a0 = c.u_s, da = c.(u - u_s),
- *   P(u) = 3a + 4.5 a^2 - 1.5 u^2,
- *   feq - s = w (drho (1 + P(u)) + rho_s (P(u) - P(u_s))),
- *   P(u) - P(u_s) = 3 da + 4.5 da (a + a0) - 1.5 (u - u_s).(u + u_s),
- * so every term is a small number and FP32 keeps its digits. */
+/* What the Guo term of a low-precision collision needs. */
+struct LpForce {
+  float ux, uy, uz, Fx, Fy, Fzg;
+};
+
+/* Guo forcing term of direction q with the FP32 constants. */
+template <typename P>
+__device__ __forceinline__ float lp_guo(int q, const LpForce& c, const P& p) {
+  const float c0 = (float)cx(q), c1 = (float)cy(q), c2 = (float)cz(q);
+  const float kw = (q == 0) ? p.fkw0 : ((q <= 6) ? p.fkw1 : p.fkw2);
+  const float A = (c0 - c.ux) * c.Fx + (c1 - c.uy) * c.Fy + (c2 - c.uz) * c.Fzg;
+  const float B = c0 * c.ux + c1 * c.uy + c2 * c.uz;
+  const float C = c0 * c.Fx + c1 * c.Fy + c2 * c.Fzg;
+  return kw * (A * p.fcs2i + B * p.fcs4i * C);
+}
+
+/* Deviation-form BGK (+ Guo) for one opposite pair (qa, qb), c_qa = -c_qb,
+ * a = c_qa.u.  With P_q(u) = 3 c.u + 4.5 (c.u)^2 - 1.5 u^2 and the shift
+ * s_q = w_q rho_s (1 + P_q(u_s)):
+ *   feq_q - s_q = w_q (drho + rho P_q(u) - C_q),  C_q = rho_s P_q(u_s),
+ * a sum of small terms (C_q is a per-direction constant), so FP32 keeps
+ * the digits the deviations carry. */
 template <bool FORCED, int QA, int QB, typename P>
-__device__ __forceinline__ void lp_relax_pair(float* d, float a, float da, float a0, float w, float drho,
-                                              float rs, float t, float td, float om, float it, float ux,
-                                              float uy, float uz, float Fx, float Fy, float Fzg, const P& p) {
+__device__ __forceinline__ void lp_pair(float* d, float a, float itw, float drho, float rho, float t, float om,
+                                        const LpForce& c, const P& p) {
   const float sq = 4.5f * a * a - t;
-  const float dq = 4.5f * da * (a + a0) - td;
-  const float ea = w * (drho * (1.0f + sq + 3.0f * a) + rs * (dq + 3.0f * da));
-  const float eb = w * (drho * (1.0f + sq - 3.0f * a) + rs * (dq - 3.0f * da));
-  float va = d[QA] * om + it * ea;
-  float vb = d[QB] * om + it * eb;
+  const float xa = (drho - p.fC[QA]) + rho * (sq + 3.0f * a);
+  const float xb = (drho - p.fC[QB]) + rho * (sq - 3.0f * a);
+  float va = d[QA] * om + itw * xa;
+  float vb = d[QB] * om + itw * xb;
   if (FORCED) {
-    va += guo(QA, ux, uy, uz, Fx, Fy, Fzg, p);
-    vb += guo(QB, ux, uy, uz, Fx, Fy, Fzg, p);
+    va += lp_guo(QA, c, p);
+    vb += lp_guo(QB, c, p);
   }
   d[QA] = va;
   d[QB] = vb;
@@ -92,6 +106,9 @@ struct Form<T, false> {
   }
   static __device__ __forceinline__ void moments(const R f[19], R Fx, R Fy, R Fz, const P& p, Mom<R>& m) {
     lbib::moments(f, Fx, Fy, Fz, p.half_dt, p.g, m.rho, m.ux, m.uy, m.uz);
+  }
+  static __device__ __forceinline__ void moments_free(const R f[19], const P& p, Mom<R>& m) {
+    lbib::moments(f, 0.0, 0.0, 0.0, p.half_dt, p.g, m.rho, m.ux, m.uy, m.uz);
   }
   template <bool FORCED>
   static __device__ __forceinline__ void collide(R f[19], const Mom<R>& m, R Fx, R Fy, R Fz, const P& p) {
@@ -126,37 +143,47 @@ struct Form<T, true> {
     const float jx = ((d[1] - d[2]) + (d[7] - d[8])) + ((d[9] - d[10]) + (d[15] - d[16])) + (d[17] - d[18]);
     const float jy = ((d[6] - d[5]) + (d[12] - d[11])) + ((d[13] - d[14]) + (d[16] - d[15])) + (d[17] - d[18]);
     const float jz = ((d[3] - d[4]) + (d[7] - d[8])) + ((d[10] - d[9]) + (d[11] - d[12])) + (d[13] - d[14]);
-    const float rs = (float)p.rhos, us = (float)p.uxs, h = (float)p.half_dt;
-    const float rho = rs + drho;
-    const float inv = 1.0f / rho;
+    const float rho = p.frs + drho;
+    const float inv = __frcp_rn(rho);
     m.rho = drho;
-    m.ux = (jx + h * Fx - drho * us) * inv;
-    m.uy = (jy + h * Fy) * inv;
-    m.uz = (jz + h * (Fz + rho * (float)p.g)) * inv;
+    m.ux = (jx + p.fhdt * Fx - drho * p.fus) * inv;
+    m.uy = (jy + p.fhdt * Fy) * inv;
+    m.uz = (jz + p.fhdt * (Fz + rho * p.fg)) * inv;
   }
   template <bool FORCED>
   static __device__ __forceinline__ void collide(R d[19], const Mom<R>& m, R Fx, R Fy, R Fz, const P& p) {
-    const float rs = (float)p.rhos, us = (float)p.uxs;
-    const float drho = m.rho, dux = m.ux, duy = m.uy, duz = m.uz;
-    const float ux = us + dux, uy = duy, uz = duz;
-    const float rho = rs + drho;
+    const float drho = m.rho, rho = p.frs + drho;
+    const float ux = p.fus + m.ux, uy = m.uy, uz = m.uz;
     const float t = 1.5f * (ux * ux + uy * uy + uz * uz);
-    const float td = 1.5f * (dux * (ux + us) + duy * uy + duz * uz);
-    const float om = (float)p.omtau, it = (float)p.invtau;
-    const float Fzg = FORCED ? Fz + rho * (float)p.g : 0.0f;
-    const float w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
-    float v0 = d[0] * om + it * ((1.0f / 3.0f) * (drho * (1.0f - t) - rs * td));
-    if (FORCED) v0 += guo(0, ux, uy, uz, Fx, Fy, Fzg, p);
+    const float om = p.fom, i1 = p.fitw1, i2 = p.fitw2;
+    LpForce c;
+    if (FORCED) { c.ux = ux; c.uy = uy; c.uz = uz; c.Fx = Fx; c.Fy = Fy; c.Fzg = Fz + rho * p.fg; }
+    float v0 = d[0] * om + p.fitw0 * ((drho - p.fC[0]) - rho * t);
+    if (FORCED) v0 += lp_guo(0, c, p);
     d[0] = v0;
-    lp_relax_pair<FORCED, 1, 2>(d, ux, dux, us, w1, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
-    lp_relax_pair<FORCED, 3, 4>(d, uz, duz, 0.0f, w1, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
-    lp_relax_pair<FORCED, 6, 5>(d, uy, duy, 0.0f, w1, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
-    lp_relax_pair<FORCED, 7, 8>(d, ux + uz, dux + duz, us, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
-    lp_relax_pair<FORCED, 9, 10>(d, ux - uz, dux - duz, us, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
-    lp_relax_pair<FORCED, 11, 12>(d, uz - uy, duz - duy, 0.0f, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
-    lp_relax_pair<FORCED, 13, 14>(d, uy + uz, duy + duz, 0.0f, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
-    lp_relax_pair<FORCED, 15, 16>(d, ux - uy, dux - duy, us, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
-    lp_relax_pair<FORCED, 17, 18>(d, ux + uy, dux + duy, us, w2, drho, rs, t, td, om, it, ux, uy, uz, Fx, Fy, Fzg, p);
+    lp_pair<FORCED, 1, 2>(d, ux, i1, drho, rho, t, om, c, p);
+    lp_pair<FORCED, 3, 4>(d, uz, i1, drho, rho, t, om, c, p);
+    lp_pair<FORCED, 6, 5>(d, uy, i1, drho, rho, t, om, c, p);
+    lp_pair<FORCED, 7, 8>(d, ux + uz, i2, drho, rho, t, om, c, p);
+    lp_pair<FORCED, 9, 10>(d, ux - uz, i2, drho, rho, t, om, c, p);
+    lp_pair<FORCED, 11, 12>(d, uz - uy, i2, drho, rho, t, om, c, p);
+    lp_pair<FORCED, 13, 14>(d, uy + uz, i2, drho, rho, t, om, c, p);
+    lp_pair<FORCED, 15, 16>(d, ux - uy, i2, drho, rho, t, om, c, p);
+    lp_pair<FORCED, 17, 18>(d, ux + uy, i2, drho, rho, t, om, c, p);
+  }
+  /* moments without force: the unforced cells' common case */
+  static __device__ __forceinline__ void moments_free(const R d[19], const P& p, Mom<R>& m) {
+    const float m0 = ((d[0] + d[1]) + (d[2] + d[3])) + ((d[4] + d[5]) + (d[6] + d[7]));
+    const float m1 = ((d[8] + d[9]) + (d[10] + d[11])) + ((d[12] + d[13]) + (d[14] + d[15]));
+    const float drho = (m0 + m1) + ((d[16] + d[17]) + d[18]);
+    const float jx = ((d[1] - d[2]) + (d[7] - d[8])) + ((d[9] - d[10]) + (d[15] - d[16])) + (d[17] - d[18]);
+    const float jy = ((d[6] - d[5]) + (d[12] - d[11])) + ((d[13] - d[14]) + (d[16] - d[15])) + (d[17] - d[18]);
+    const float jz = ((d[3] - d[4]) + (d[7] - d[8])) + ((d[10] - d[9]) + (d[11] - d[12])) + (d[13] - d[14]);
+    const float inv = __frcp_rn(p.frs + drho);
+    m.rho = drho;
+    m.ux = (jx - drho * p.fus) * inv;
+    m.uy = jy * inv;
+    m.uz = jz * inv;
   }
   static __device__ __forceinline__ void to_double(const Mom<R>& m, const P& p, double& rho, double& ux,
                                                    double& uy, double& uz) {
@@ -168,15 +195,10 @@ struct Form<T, true> {
   }
 };
 
+/* One cell of I through the generic rules: load, moments, collision, store. */
 template <typename T, int PAR>
-__global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
-    lbib_fluid_step(FluidParamsT<T> p, const int2* __restrict__ rows) {
+__device__ __forceinline__ void step_cell(const FluidParamsT<T>& p, int x, int y, int z) {
   using R = typename Pop<T>::R;
-  const int x = blockIdx.y * blockDim.x + threadIdx.x + 2;
-  const int2 r = rows[blockIdx.x];
-  const int y = r.x;
-  const int z = r.y;
-  if (x > p.nx - 3) return;
   const long idx = ((long)z * p.ny + y) * p.nx + x;
   const int kind = classify(p, x, y, z);
   R f[19];
@@ -190,7 +212,7 @@ __global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
   } else {
     const int sp = p.slot_prev[tile];
     if (sp >= 0) F::from_tile(p, p.Uprev + (long)sp * 256, cell, m);
-    else F::moments(f, R(0), R(0), R(0), p, m);
+    else F::moments_free(f, p, m);
   }
   const int sc = p.slot_cur[tile];
   if (sc >= 0) {
@@ -200,6 +222,15 @@ __global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
     F::template collide<false>(f, m, R(0), R(0), R(0), p);
   }
   store_post<PAR>(p, x, y, z, idx, kind, f);
+}
+
+template <typename T, int PAR>
+__global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
+    lbib_fluid_step(FluidParamsT<T> p, const int2* __restrict__ rows) {
+  const int x = blockIdx.y * blockDim.x + threadIdx.x + 2;
+  const int2 r = rows[blockIdx.x];
+  if (x > p.nx - 3) return;
+  step_cell<T, PAR>(p, x, r.x, r.y);
 }
 
 /* (rho, u)(t) of every cell of the touched tiles, after the fused step of
@@ -361,6 +392,15 @@ FluidParamsT<T> make_params_t(lbib_device* d, int first) {
   p.slot_prev = d->tile_slot[c ^ 1]; p.Uprev = d->Utile[c ^ 1];
   p.ntx = d->ntx; p.nty = d->nty;
   lbdev_shift(d, p.sh, &p.rhos, &p.uxs);
+  p.frs = (float)p.rhos; p.fus = (float)p.uxs;
+  p.fom = (float)p.omtau; p.fit = (float)p.invtau; p.fhdt = (float)p.half_dt; p.fg = (float)p.g;
+  p.fkw0 = (float)p.kw0; p.fkw1 = (float)p.kw1; p.fkw2 = (float)p.kw2;
+  p.fcs2i = (float)(1.0 / p.cs2); p.fcs4i = (float)(1.0 / p.cs4);
+  p.fitw0 = (float)(p.invtau / 3.0); p.fitw1 = (float)(p.invtau / 18.0); p.fitw2 = (float)(p.invtau / 36.0);
+  for (int q = 0; q < 19; ++q) {
+    const double a0 = cx(q) * p.uxs;
+    p.fC[q] = (float)(p.rhos * (3.0 * a0 + 4.5 * a0 * a0 - 1.5 * p.uxs * p.uxs));
+  }
   return p;
 }
 

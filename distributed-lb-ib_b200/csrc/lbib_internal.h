@@ -67,7 +67,8 @@ typedef struct lbib_device {
   void* outlet;
   int parity;
   long steps;                    /* fused steps since init_df1               */
-  int use_bulk;                  /* staged kernel for rows away from walls   */
+  int use_bulk;                  /* bulk kernel for rows away from walls     */
+  int lp_variant;                /* low-precision word-kernel variant, -1 = default */
   int* rows;                     /* device int2 (y, z) rows of the generic kernel */
   int nrows;
   int have_eq, have_df1, have_inout;
@@ -140,6 +141,12 @@ int  lbdev_conservation(lbib_device* d, double* out);
 int  lbdev_get_nodes(lbib_device* d, double* out);
 int  lbdev_set_nodes(lbib_device* d, const double* in);
 int  lbdev_sync(lbib_device* d);
+int  lbdev_variants(const lbib_device* d);     /* kernel variants for this precision */
+int  lbdev_set_variant(lbib_device* d, int v);
+/* Times every variant on fluid steps from the initial state, keeps the
+ * fastest, and restores the initial populations; only before the first
+ * step.  ms[i] = mean ms per step of variant i (ms may be NULL). */
+int  lbdev_autotune(lbib_device* d, int steps, double* ms, int max_ms, int* best);
 int  lbdev_profile_begin(lbib_device* d);
 int  lbdev_profile_end(lbib_device* d, double* stage_ms, long* steps);
 

@@ -106,6 +106,13 @@ struct FluidParamsT {
   int ntx, nty;
   float sh[19];
   double rhos, uxs;
+  /* the same constants in FP32 for the low-precision forms: rho_s, u_s,
+     1 - 1/tau, 1/tau, dt/2, g, the Guo weights, 1/cs^2, 1/cs^4 */
+  float frs, fus, fom, fit, fhdt, fg, fkw0, fkw1, fkw2, fcs2i, fcs4i;
+  /* 1/tau times the weights, and C_q = rho_s P_q(u_s) (the shift's part of
+     the deviation equilibrium) */
+  float fitw0, fitw1, fitw2;
+  float fC[19];
 };
 
 /* A bounce-back link delivers this cell's own outgoing population opp(q) as

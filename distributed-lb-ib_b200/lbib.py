@@ -51,6 +51,7 @@ EXPORTED = [
     "lbib_run", "lbib_synchronize", "lbib_stream", "lbib_case_create", "lbib_case_free", "lbib_stage",
     "lbib_device_count", "lbib_kernel_launches", "lbib_profile_begin", "lbib_profile_end",
     "lbib_set_precision", "lbib_case_create_prec", "lbib_spread_force_noalloc", "lbib_conservation_sums",
+    "lbib_kernel_variants", "lbib_set_kernel_variant", "lbib_autotune",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -94,6 +95,9 @@ def load() -> C.CDLL:
     lib.lbib_get_force.argtypes = [C.c_void_p] + [_dp] * 3
     lib.lbib_get_df1.argtypes = [C.c_void_p, _dp]
     lib.lbib_conservation_sums.argtypes = [C.c_void_p, _dp]
+    lib.lbib_kernel_variants.argtypes = [C.c_void_p]
+    lib.lbib_set_kernel_variant.argtypes = [C.c_void_p, C.c_int]
+    lib.lbib_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
     lib.lbib_get_sheet.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.lbib_set_sheet.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.lbib_synchronize.argtypes = [C.c_void_p]
@@ -228,6 +232,22 @@ class Solver:
         a = np.empty(19 * self.N)
         _check(self.lib.lbib_get_df1(self.gv, _ptr(a)), "lbib_get_df1")
         return a.reshape(19, c.nz, c.ny, c.nx)
+
+    def variants(self) -> int:
+        n = self.lib.lbib_kernel_variants(self.gv)
+        _check(min(n, 0), "lbib_kernel_variants")
+        return n
+
+    def set_variant(self, v: int) -> None:
+        _check(self.lib.lbib_set_kernel_variant(self.gv, v), "lbib_set_kernel_variant")
+
+    def autotune(self, steps: int = 8):
+        """Pick the fastest fluid-kernel variant (before the first step).
+        Returns (chosen variant, ms per step of each variant)."""
+        ms = np.zeros(max(self.variants(), 1))
+        best = self.lib.lbib_autotune(self.gv, steps, _ptr(ms), len(ms))
+        _check(min(best, 0), "lbib_autotune")
+        return best, ms.tolist()
 
     def conservation(self) -> np.ndarray:
         """[mass, x, y, z momentum] of the populations, FP64 fixed-order sums."""

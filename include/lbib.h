@@ -268,6 +268,18 @@ int lbib_set_compat(GV gv, int flags);
  * init_df1 and init_df_inout after).  LBIB_E_STATE once sheets are
  * uploaded, LBIB_E_ARG for an unknown value. */
 int lbib_set_precision(GV gv, int precision);
+/* Kernel variants of the fluid step for the grid's precision (the
+ * low-precision forms have several -- cells per thread, register budget,
+ * prefetch -- FP64 has one), and choosing among them.  lbib_autotune times
+ * every variant on `steps` fluid steps from the initial state, keeps the
+ * fastest and restores the initial populations, so the run is unchanged;
+ * call it after init_df1 / init_df_inout and before the first step.  It
+ * returns the chosen variant (>= 0) or an error code; ms_per_variant[i]
+ * (up to max_variants entries, may be NULL) gets each variant's mean ms per
+ * step. */
+int lbib_kernel_variants(GV gv);
+int lbib_set_kernel_variant(GV gv, int variant);
+int lbib_autotune(GV gv, int steps, double* ms_per_variant, int max_variants);
 int lbib_last_error(void);
 const char* lbib_error_string(int code);
 void lbib_clear_error(void);

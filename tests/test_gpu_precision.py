@@ -106,3 +106,63 @@ def test_precision_switch_rebuilds_state(gpu):
         lib.lbib_clear_error()
         assert lib.lbib_set_precision(s.gv, lbib.PREC_F32) == -4  # sheets already uploaded
         lib.lbib_clear_error()
+
+
+# cases for the word kernel: rows of 3+ warps (lane 0 / 31 crossings), a row
+# of one active word (nx = 12), forcing tiles at the row ends
+WORD_CASES = {
+    "long_rows": (small_case(160, 12, 12, 6, 6, 20.0), 9),
+    "short_rows": (small_case(12, 12, 24, 6, 6, 5.0), 7),
+    "sheet_at_inlet": (small_case(32, 16, 16, 8, 8, 4.5), 9),
+}
+# rounding-level differences only: FMA contraction may differ between the
+# two kernels, which moves a 16-bit value by at most an ulp now and then
+WORD_TOL = {"f32": 1e-9, "f32-flow": 1e-9, "f16": 2e-6, "f16-flow": 2e-6, "bf16": 2e-5, "bf16-flow": 2e-5}
+
+
+def _run(case, prec, steps, monkeypatch, bulk, variant=-1):
+    if bulk:
+        monkeypatch.delenv("LBIB_FLUID_BULK", raising=False)
+    else:
+        monkeypatch.setenv("LBIB_FLUID_BULK", "0")
+    with lbib.Solver(case, prec) as s:
+        s.set_variant(variant)
+        s.run(steps)
+        return s.df1()[interior(case)], s.moments(), s.sheet(0)
+
+
+@pytest.mark.parametrize("prec", LP)
+@pytest.mark.parametrize("name", sorted(WORD_CASES))
+def test_word_kernel_matches_cell_kernel(gpu, monkeypatch, prec, name):
+    """Every variant of the multi-cell word kernel against the one-cell
+    generic kernel, over both AA parities."""
+    case, steps = WORD_CASES[name]
+    b = _run(case, prec, steps, monkeypatch, False)
+    with lbib.Solver(case, prec) as s:
+        nv = s.variants()
+    assert nv >= 4
+    for v in range(nv):
+        a = _run(case, prec, steps, monkeypatch, True, v)
+        assert np.max(np.abs(a[0] - b[0])) <= WORD_TOL[prec], v
+        for x, y in zip(a[1], b[1]):
+            assert np.max(np.abs(x - y)) <= 50 * WORD_TOL[prec], v
+        assert np.max(np.abs(a[2] - b[2])) <= 1e-6, v
+
+
+def test_autotune_leaves_the_run_unchanged(gpu):
+    case = small_case(64, 16, 16, 8, 8, 10.0)
+    with lbib.Solver(case, "f16-flow") as s:
+        best, ms = s.autotune(4)
+        assert 0 <= best < s.variants() and len(ms) == s.variants() and min(ms) > 0
+        s.run(6)
+        a = s.df1()
+    with lbib.Solver(case, "f16-flow") as s:
+        s.set_variant(best)
+        s.run(6)
+        b = s.df1()
+    np.testing.assert_array_equal(a, b)
+    with lbib.Solver(case, "f16-flow") as s:
+        s.run(1)
+        lib = lbib.load()
+        assert lib.lbib_autotune(s.gv, 4, None, 0) == -4   # only before the first step
+        lib.lbib_clear_error()
