@@ -282,12 +282,21 @@ def run_reference(args):
     return 0
 
 
+def pop_bytes(precision):
+    return {"f64": 8, "f32": 4}.get(precision.split("-")[0], 2)
+
+
 def config_block(args):
     c = CONFIGS[args.config]
-    return {"workload": f"{args.config}: FP64 LBM-IB step, {c['nx']}x{c['ny']}x{c['nz']} D3Q19 lattice, "
+    prec = getattr(args, "precision", "f64")
+    store = "FP64" if prec == "f64" else f"{prec} storage / FP32 arithmetic"
+    gb = c["nx"] * c["ny"] * c["nz"] * 19 * pop_bytes(prec) / 1e9
+    return {"workload": f"{args.config}: {store} LBM-IB step, {c['nx']}x{c['ny']}x{c['nz']} D3Q19 lattice, "
                         f"{c['rows']}x{c['cols']} fiber sheet at x={c['x0']:g}, tau 0.6, u 0.01, Ks 0.05, Kb 0.005",
             "lattice": [c["nx"], c["ny"], c["nz"]], "sheet": [c["rows"], c["cols"]],
-            "parallelism": f"replicas x{args.gpus}", "l2_flush": "inputs (5.1 GB populations) >> L2"}
+            "parallelism": f"replicas x{args.gpus}",
+            "l2_flush": f"inputs ({gb:.2f} GB populations) vs 126 MB L2" + (" -- larger, no flush needed"
+                                                                              if gb > 0.5 else "")}
 
 
 # ---------------------------------------------------------------- GPU leg
@@ -335,12 +344,16 @@ def run_lbib(args):
     value = whole_job_mlups(case.ncells, args.steps, world, ms_max / 1e3)
 
     fluid_cells = (case.nx - 4) * (case.ny - 4) * (case.nz - 4)
-    pop_bytes = {"f64": 8, "f32": 4}.get(args.precision.split("-")[0], 2)
-    bytes_launch = fluid_cells * 19 * 2 * pop_bytes
+    bytes_launch = fluid_cells * 19 * 2 * pop_bytes(args.precision)
     fluid_ms = stage_ms["fluid"] / max(nprof, 1)
     achieved = bytes_launch / (fluid_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = profile_traffic()
+
+    # ---- the FP16-store form of the same workload, same step count
+    lp = None
+    if args.precision == "f64" and args.lp_form != "none":
+        lp = run_lp_form(args, case, solver, group, value, peak)
 
     # ---- end to end through the C ABI with host buffers
     S = sum(s.rows * s.cols for s in case.sheets)
@@ -377,18 +390,69 @@ def run_lbib(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "f64" else f"{args.precision} storage, f32 arithmetic",
+                "data": "synthetic",
                 "config": config_block(args),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                              "kernel": "lbib_fluid_step (fused D3Q19 AA step)",
                              "bytes_per_launch": bytes_launch, "launch_ms": fluid_ms},
                 "stages_ms_per_step": {k: v / max(nprof, 1) for k, v in stage_ms.items()},
-                "gpu_launches": launches, "autotune": tuned,
+                "gpu_launches": launches, "autotune": tuned, "fp16_store": lp,
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)
     group.close()
     return 0
+
+
+def run_lp_form(args, case, ref_solver, group, value64, peak):
+    """Time the low-precision storage form (default f16-flow: FP16 deviations
+    from the inflow equilibrium, FP32 arithmetic) on the same workload and
+    step count as the FP64 leg, and state its error against that FP64 state."""
+    import numpy as np
+    import torch
+
+    import lbib
+    import precision
+    s = lbib.Solver(case, precision=args.lp_form)
+    sheet0 = s.sheet(0)
+    best, ms_v = s.autotune(8)
+    stream = torch.cuda.ExternalStream(s.stream)
+    s.run(args.warmup)
+    s.synchronize()
+    group.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.profile_begin()
+    e0.record(stream)
+    s.run(args.steps)
+    e1.record(stream)
+    stage_ms, nprof = s.profile_end()
+    torch.cuda.synchronize()
+    ms = group.max(e0.elapsed_time(e1))
+    world = group.world
+    v = whole_job_mlups(case.ncells, args.steps, world, ms / 1e3)
+    fluid_cells = (case.nx - 4) * (case.ny - 4) * (case.nz - 4)
+    pop = pop_bytes(args.lp_form)
+    fluid_ms = stage_ms["fluid"] / max(nprof, 1)
+    achieved = fluid_cells * 19 * 2 * pop / (fluid_ms / 1e3) / 1e9
+    # error against the FP64 leg, which has run the same warmup + steps
+    u64 = np.stack(ref_solver.moments()[1:])
+    ulp = np.stack(s.moments()[1:])
+    sl = (slice(None), slice(2, case.nz - 2), slice(2, case.ny - 2), slice(2, case.nx - 2))
+    vel = float(np.linalg.norm(ulp[sl] - u64[sl]) / np.linalg.norm(u64[sl]))
+    d64 = precision.tip_displacement(sheet0, ref_solver.sheet(0))
+    dlp = precision.tip_displacement(sheet0, s.sheet(0))
+    s.close()
+    return {"form": args.lp_form, "value": v, "unit": UNIT, "ms_per_step": ms / args.steps,
+            "speedup_vs_f64": v / value64,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "bytes_per_launch": fluid_cells * 19 * 2 * pop,
+                         "launch_ms": fluid_ms},
+            "stages_ms_per_step": {k: x / max(nprof, 1) for k, x in stage_ms.items()},
+            "autotune": {"variant": best, "ms_per_step": ms_v},
+            "error_vs_f64": {"steps": args.warmup + args.steps, "velocity_rel_l2": vel,
+                             "tip_displacement_rel": abs(dlp - d64) / max(abs(d64), 1e-300)}}
 
 
 def main():
@@ -401,6 +465,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lp-form", default="f16-flow",
+                    help="low-precision form timed beside the FP64 leg (or 'none')")
     ap.add_argument("--variant", type=int, default=None,
                     help="fluid-kernel variant (default: autotuned when there are several)")
     ap.add_argument("--precision", default="f64",
