@@ -1,0 +1,131 @@
+/*
+ * Batched fluid kernels: many independent problems of uneven size advanced
+ * by one launch per stage.
+ *
+ * Every problem keeps its own populations, tables and parameters (a
+ * FluidParamsT<T> per problem in device memory, whose pointers reach into
+ * the batch's pools); its tiles are a slice [tile0, tile0 + ntiles) of one
+ * global tile space, so one touched-tile list, one slot space and one
+ * compaction serve the whole batch.  Work is enumerated across problems:
+ *   rows     (problem, y, z) of the rows the generic kernel takes;
+ *   words    blocks of the word kernel, (problem, block within problem);
+ *   edges    the cells x in {2, 3, nx-4, nx-3} of bulk rows, as a prefix
+ *            over problems;
+ *   tiles    the global touched-tile list, tile -> problem by a table.
+ * A problem whose error word is set (a fiber stencil left its grid) is
+ * skipped by every kernel from then on; the others continue.
+ *
+ * The per-cell arithmetic is the one-grid code (step_cell, words_item,
+ * tile_moments_cell), so a problem advanced in a batch gets the same
+ * numbers as the same problem on its own.
+ */
+#ifndef LBIB_BATCH_CUH
+#define LBIB_BATCH_CUH
+
+#include "lbib_words.cuh"
+
+namespace lbib {
+
+/* What the node- and tile-level kernels need of a problem. */
+struct BatchDesc {
+  int nx, ny, nz, ntx, nty;
+  int rows, cols;          /* its one sheet */
+  int bulk;                /* bulk rows run the word kernel */
+  long tile0, ntiles;      /* slice of the global tile space */
+  long node0, S;           /* nodes [node0, node0 + S); node0 % 32 == 0 */
+  double bc, sc, sc2, ds1, ds2, dt;
+};
+
+/* Copy a parameter struct into shared memory with the whole block. */
+template <typename S>
+__device__ __forceinline__ void block_copy(S& dst, const S* __restrict__ src) {
+  static_assert(sizeof(S) % 4 == 0, "word copy");
+  const uint32_t* a = reinterpret_cast<const uint32_t*>(src);
+  uint32_t* b = reinterpret_cast<uint32_t*>(&dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(S) / 4); i += blockDim.x) b[i] = a[i];
+  __syncthreads();
+}
+
+/* Generic rows: one block per (problem, y, z) row and 128 x cells. */
+template <typename T, int PAR>
+__global__ void __launch_bounds__(128) lbib_b_rows(const FluidParamsT<T>* __restrict__ P, const int4* __restrict__ rows,
+                                                   const int* __restrict__ err) {
+  __shared__ __align__(16) FluidParamsT<T> sp;
+  const int4 r = rows[blockIdx.x];
+  if (err[2 * r.x]) return;
+  block_copy(sp, P + r.x);
+  const int x = blockIdx.y * blockDim.x + threadIdx.x + 2;
+  if (x > sp.nx - 3) return;
+  step_cell<T, PAR>(sp, x, r.y, r.z);
+}
+
+/* Word kernel over the blocks of all problems that run it. */
+template <typename T, int V, int PAR, int MINB>
+__global__ void __launch_bounds__(WTPB, MINB) lbib_b_words(const WordsParams<T>* __restrict__ WP,
+                                                           const int2* __restrict__ blk, const int* __restrict__ err) {
+  __shared__ __align__(16) WordsParams<T> sb;
+  const int2 m = blk[blockIdx.x];
+  if (err[2 * m.x]) return;
+  block_copy(sb, WP + m.x);
+  words_item<T, V, PAR>(sb, (long)m.y * WTPB + threadIdx.x);
+}
+
+/* Largest i with off[i] <= t (off ascending, off[0] = 0, n entries). */
+__device__ __forceinline__ int find_slice(const long* __restrict__ off, int n, long t) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+/* Edge cells: thread t -> problem by the prefix edge_off[0..B] of 4 * bulk
+ * rows per problem. */
+template <typename T, int PAR>
+__global__ void __launch_bounds__(128) lbib_b_edges(const FluidParamsT<T>* __restrict__ P,
+                                                    const WordsParams<T>* __restrict__ WP,
+                                                    const long* __restrict__ edge_off, int B, const int* __restrict__ err) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= edge_off[B]) return;
+  const int k = find_slice(edge_off, B + 1, t);
+  if (err[2 * k] || edge_off[k + 1] == edge_off[k]) return;
+  const long e = t - edge_off[k];
+  edge_cell<T, PAR>(P[k], WP[k].nry, (int)(e >> 2), (int)(e & 3));
+}
+
+/* Cells of forced tiles in the word kernel's range, over the global list. */
+template <typename T, int PAR>
+__global__ void __launch_bounds__(64) lbib_b_forced(const FluidParamsT<T>* __restrict__ P,
+                                                    const BatchDesc* __restrict__ D, const int* __restrict__ list,
+                                                    const int* __restrict__ count, const int* __restrict__ tile_inst,
+                                                    const int* __restrict__ err) {
+  const int n = *count;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int tile = list[i];
+    const int k = tile_inst[tile];
+    if (err[2 * k] || !D[k].bulk) continue;
+    const FluidParamsT<T>& p = P[k];
+    const int zb = min(p.nz - 4, p.zin_hi);
+    forced_cell<T, PAR>(p, (int)(tile - D[k].tile0), threadIdx.x, zb);
+  }
+}
+
+/* (rho, u) of the touched tiles, over the global list. */
+template <typename T, int PAR>
+__global__ void lbib_b_tile_moments(const FluidParamsT<T>* __restrict__ P, const BatchDesc* __restrict__ D,
+                                    const int* __restrict__ list, const int* __restrict__ count,
+                                    const int* __restrict__ tile_inst, const double* __restrict__ Ftile,
+                                    double* __restrict__ Utile, const int* __restrict__ err) {
+  const int n = *count;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int tile = list[i];
+    const int k = tile_inst[tile];
+    if (err[2 * k]) continue;
+    tile_moments_cell<T, PAR>(P[k], (int)(tile - D[k].tile0), i, threadIdx.x, Ftile, Utile);
+  }
+}
+
+}  // namespace lbib
+
+#endif

@@ -1,0 +1,108 @@
+/*
+ * Low-precision fluid kernels of the batched step (FP32 / FP16 / BF16
+ * deviations, FP32 arithmetic; FMA contraction allowed, as in
+ * lbib_fluid_lp.cu): instantiations of lbib_batch.cuh.
+ */
+#include "lbib_batch.cuh"
+#include "lbib_batch_internal.h"
+
+namespace lbib {
+
+namespace {
+
+template <typename T>
+int rest(const BatchFluid& f) {
+  const FluidParamsT<T>* P = static_cast<const FluidParamsT<T>*>(f.P);
+  const WordsParams<T>* WP = static_cast<const WordsParams<T>*>(f.WP);
+  if (f.nrows > 0) {
+    dim3 grid((unsigned)f.nrows, (unsigned)((f.max_nx - 4 + 127) / 128));
+    if (f.par == 0) lbib_b_rows<T, 0><<<grid, 128, 0, f.stream>>>(P, f.rows, f.err);
+    else lbib_b_rows<T, 1><<<grid, 128, 0, f.stream>>>(P, f.rows, f.err);
+  }
+  if (f.nedge > 0) {
+    const unsigned eb = (unsigned)((f.nedge + 127) / 128);
+    if (f.par == 0) lbib_b_edges<T, 0><<<eb, 128, 0, f.stream>>>(P, WP, f.edge_off, f.B, f.err);
+    else lbib_b_edges<T, 1><<<eb, 128, 0, f.stream>>>(P, WP, f.edge_off, f.B, f.err);
+  }
+  if (f.par == 0) lbib_b_forced<T, 0><<<f.grid_tiles, 64, 0, f.stream>>>(P, f.desc, f.list, f.count, f.tile_inst, f.err);
+  else lbib_b_forced<T, 1><<<f.grid_tiles, 64, 0, f.stream>>>(P, f.desc, f.list, f.count, f.tile_inst, f.err);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename T, int V, int MINB>
+int words(const BatchFluid& f, const int2* blk, long nblk) {
+  if (nblk <= 0) return 0;
+  const WordsParams<T>* WP = static_cast<const WordsParams<T>*>(f.WP);
+  if (f.par == 0) lbib_b_words<T, V, 0, MINB><<<(unsigned)nblk, WTPB, 0, f.stream>>>(WP, blk, f.err);
+  else lbib_b_words<T, V, 1, MINB><<<(unsigned)nblk, WTPB, 0, f.stream>>>(WP, blk, f.err);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+/* The one-grid autotuner's table: 16-bit {V, MINB} = {4,3} {4,4} {2,4}
+ * {2,5} {2,6}; FP32 {2,3} {2,4} {2,5}. */
+template <typename T>
+int words_v(const BatchFluid& f, int v, const int2* blk, long nblk) {
+  if constexpr (sizeof(T) == 2) {
+    switch (v) {
+      case 1: return words<T, 4, 4>(f, blk, nblk);
+      case 2: return words<T, 2, 4>(f, blk, nblk);
+      case 3: return words<T, 2, 5>(f, blk, nblk);
+      case 4: return words<T, 2, 6>(f, blk, nblk);
+      default: return words<T, 4, 3>(f, blk, nblk);
+    }
+  } else {
+    switch (v) {
+      case 1: return words<T, 2, 4>(f, blk, nblk);
+      case 2: return words<T, 2, 5>(f, blk, nblk);
+      default: return words<T, 2, 3>(f, blk, nblk);
+    }
+  }
+}
+
+template <typename T>
+int moments(const BatchFluid& f) {
+  const FluidParamsT<T>* P = static_cast<const FluidParamsT<T>*>(f.P);
+  if (f.par == 0)
+    lbib_b_tile_moments<T, 0><<<f.grid_tiles, 64, 0, f.stream>>>(P, f.desc, f.list, f.count, f.tile_inst, f.Ftile, f.Utile, f.err);
+  else
+    lbib_b_tile_moments<T, 1><<<f.grid_tiles, 64, 0, f.stream>>>(P, f.desc, f.list, f.count, f.tile_inst, f.Ftile, f.Utile, f.err);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace
+
+int batch_fluid_rest_lp(const BatchFluid& f) {
+  switch (LBIB_PREC_TYPE(f.prec)) {
+    case LBIB_PREC_F32: return rest<float>(f);
+    case LBIB_PREC_F16: return rest<__half>(f);
+    case LBIB_PREC_BF16: return rest<__nv_bfloat16>(f);
+    default: return -1;
+  }
+}
+
+int batch_words_lp(const BatchFluid& f, int variant, const int2* blk, long nblk) {
+  switch (LBIB_PREC_TYPE(f.prec)) {
+    case LBIB_PREC_F32: return words_v<float>(f, variant, blk, nblk);
+    case LBIB_PREC_F16: return words_v<__half>(f, variant, blk, nblk);
+    case LBIB_PREC_BF16: return words_v<__nv_bfloat16>(f, variant, blk, nblk);
+    default: return -1;
+  }
+}
+
+int batch_variants_lp(int prec) { return LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? 3 : 5; }
+
+int batch_variant_cells_lp(int prec, int variant) {
+  if (LBIB_PREC_TYPE(prec) == LBIB_PREC_F32) return 2;
+  return (variant == 0 || variant == 1) ? 4 : 2;
+}
+
+int batch_tile_moments_lp(const BatchFluid& f) {
+  switch (LBIB_PREC_TYPE(f.prec)) {
+    case LBIB_PREC_F32: return moments<float>(f);
+    case LBIB_PREC_F16: return moments<__half>(f);
+    case LBIB_PREC_BF16: return moments<__nv_bfloat16>(f);
+    default: return -1;
+  }
+}
+
+}  // namespace lbib

@@ -237,13 +237,10 @@ __global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
  * parity 1-PAR: compute_rho_and_u (lbm_ib.c:2440-2538) restricted to where
  * moveFiberSheet will read.  Cells outside M keep the initial values. */
 template <typename T, int PAR>
-__global__ void lbib_tile_moments(FluidParamsT<T> p, const int* __restrict__ list, const int* __restrict__ count,
-                                  const double* __restrict__ Ftile, double* __restrict__ Utile) {
+__device__ __forceinline__ void tile_moments_cell(const FluidParamsT<T>& p, int tile, int i, int cell,
+                                                  const double* __restrict__ Ftile, double* __restrict__ Utile) {
   using R = typename Pop<T>::R;
-  const int n = *count;
-  const int cell = threadIdx.x;
-  for (int i = blockIdx.x; i < n; i += gridDim.x) {
-    const int tile = list[i];
+  {
     const int tx = tile % p.ntx, ty = (tile / p.ntx) % p.nty, tz = tile / (p.ntx * p.nty);
     const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
     double rho = p.rho0, ux = p.ux0, uy = 0.0, uz = 0.0;
@@ -259,6 +256,14 @@ __global__ void lbib_tile_moments(FluidParamsT<T> p, const int* __restrict__ lis
     double* U = Utile + (long)i * 256;
     U[cell] = rho; U[64 + cell] = ux; U[128 + cell] = uy; U[192 + cell] = uz;
   }
+}
+
+/* Slot i of the touched-tile list: tile list[i]. */
+template <typename T, int PAR>
+__global__ void lbib_tile_moments(FluidParamsT<T> p, const int* __restrict__ list, const int* __restrict__ count,
+                                  const double* __restrict__ Ftile, double* __restrict__ Utile) {
+  const int n = *count;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) tile_moments_cell<T, PAR>(p, list[i], i, threadIdx.x, Ftile, Utile);
 }
 
 /* Dense rho, u over the whole grid as the reference holds them after the

@@ -1,434 +1,63 @@
 /*
- * Immersed-boundary kernels.
- *
- *   lbib_fiber_forces   compute_bendingforce + compute_stretchingforce +
- *                       compute_elasticforce (cube_pthread/lbm_ib.c:961-1318),
- *                       one thread per node, both passes of each force in
- *                       the reference's order.
- *   lbib_node_prep      per node: stencil start floor(X - 2) + 1 per axis, the
- *                       twelve delta-kernel factors 1 + cos(pi/2 r) (shared by
- *                       the spread and the interpolation of the step), the 4^3
- *                       tiles the stencil touches, and per 32-node chunk the
- *                       bounding box of its stencils.
- *   lbib_compact_*      touched tiles -> dense list in tile order, tile -> slot
- *                       map, and each slot's node-list offset (deterministic
- *                       prefix sums); lbib_pair_scatter fills the lists.
- *   lbib_spread_gather  fiber_SpreadForce + fluid_get_SpreadForce
- *                       (lbm_ib.c:1323-1525) as a gather: one CTA per touched
- *                       tile sorts the tile's node list by node index in
- *                       shared memory, then each thread (cell) sums the
- *                       contributions in that order -- the reference's
- *                       (sheet, row, col) order -- so the result is
- *                       deterministic and needs no atomics on forces.
- *   lbib_move_nodes     moveFiberSheet (lbm_ib.c:2540-2723): one thread per
- *                       node sums u * w over its 64 stencil cells in the
- *                       reference's (x, y, z) order, then X += dt U.
- * All arithmetic keeps the reference's operation order; compile with
- * -fmad=false.
+ * Immersed-boundary kernels of one grid: thin wrappers over the device code
+ * of lbib_ib.cuh (fiber forces, node preparation, the deterministic spread
+ * as a per-tile gather, interpolation and move) and their launchers.
+ * Compiled with -fmad=false: every expression keeps the reference's
+ * operation order.
  */
-#include "lbib_cos.h"
-#include "lbib_internal.h"
-#include "lbib_lattice.cuh"
+#include "lbib_ib.cuh"
+
+using namespace lbib;
 
 namespace {
-
-/* PI as truncated in the reference, cube_pthread/lbm_ib.c:33. */
-constexpr double kPi = 3.14159265358979;
-
-__device__ __forceinline__ void set_error(int* err, int code, int step) {
-  if (atomicCAS(err, 0, code) == 0) err[1] = step;
-}
 
 __global__ void lbib_fiber_forces(double* __restrict__ nodes, int R, int C, double bc, double sc, double sc2,
                                   double ds1, double ds2, int bend_bug) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= R * C) return;
-  const int r = i / C, c = i % C;
-#define P(rr, cc) (nodes + ((long)(rr) * C + (cc)) * 12)
-  const double* m = P(r, c);
-  double b[3], s[3];
-  /* bending along the fiber (row), lbm_ib.c:1002-1052 */
-  for (int d = 0; d < 3; ++d) {
-    if (c == 0) {
-      b[d] = bc * (-P(r, 2)[d] + 2 * P(r, 1)[d] - P(r, 0)[d]);
-    } else if (c == 1) {
-      b[d] = bc * (-P(r, 3)[d] + 4 * P(r, 2)[d] - 5 * P(r, 1)[d] + 2 * P(r, 0)[d]);
-    } else if (c == C - 1) {
-      b[d] = bc * (-P(r, c)[d] + 2 * P(r, c - 1)[d] - P(r, c - 2)[d]);
-    } else if (c == C - 2) {
-      const double last = (d == 0 && bend_bug) ? P(r, c)[d] : P(r, c - 2)[d];
-      b[d] = bc * (2 * P(r, c + 1)[d] - 5 * P(r, c)[d] + 4 * P(r, c - 1)[d] - last);
-    } else {
-      b[d] = bc * (-P(r, c + 2)[d] + 4.0 * P(r, c + 1)[d] - 6.0 * P(r, c)[d] + 4.0 * P(r, c - 1)[d] - P(r, c - 2)[d]);
-    }
-  }
-  /* bending across fibers (column), lbm_ib.c:1062-1145 */
-  for (int d = 0; d < 3; ++d) {
-    double v;
-    if (r == 0) {
-      v = bc * (-P(2, c)[d] + 2 * (P(1, c)[d]) - (P(0, c)[d]));
-    } else if (r == 1) {
-      v = bc * (-P(3, c)[d] + 4 * (P(2, c)[d]) - 5 * (P(1, c)[d]) + 2 * (P(0, c)[d]));
-    } else if (r == R - 1) {
-      v = bc * (-(P(r, c)[d]) + 2 * (P(r - 1, c)[d]) - (P(r - 2, c)[d]));
-    } else if (r == R - 2) {
-      v = bc * (2 * P(r + 1, c)[d] - 5 * (P(r, c)[d]) + 4 * (P(r - 1, c)[d]) - (P(r - 2, c)[d]));
-    } else {
-      v = bc * (-P(r + 2, c)[d] + 4.0 * (P(r + 1, c)[d]) - 6.0 * (P(r, c)[d]) + 4.0 * (P(r - 1, c)[d]) - (P(r - 2, c)[d]));
-    }
-    b[d] = b[d] + v;
-  }
-  /* stretching along the fiber (row), lbm_ib.c:1179-1221 */
-  if (c == 0) {
-    const double* p = P(r, 1);
-    const double t0 = p[0] - m[0], t1 = p[1] - m[1], t2 = p[2] - m[2];
-    const double dr = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
-    s[0] = sc * ((dr - ds1) * (t0 / dr));
-    s[1] = sc * ((dr - ds1) * (t1 / dr));
-    s[2] = sc * ((dr - ds1) * (t2 / dr));
-  } else if (c == C - 1) {
-    const double* q = P(r, C - 2);
-    const double t0 = m[0] - q[0], t1 = m[1] - q[1], t2 = m[2] - q[2];
-    const double dl = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
-    s[0] = sc * ((dl - ds1) * (t0 / dl));
-    s[1] = sc * ((dl - ds1) * (t1 / dl));
-    s[2] = sc * ((dl - ds1) * (t2 / dl));
-  } else {
-    const double* p = P(r, c + 1);
-    const double* q = P(r, c - 1);
-    const double r0 = p[0] - m[0], r1 = p[1] - m[1], r2 = p[2] - m[2];
-    const double l0 = q[0] - m[0], l1 = q[1] - m[1], l2 = q[2] - m[2];
-    const double dr = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
-    const double dl = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
-    s[0] = sc * ((dr - ds1) * (r0 / dr) + (dl - ds1) * (l0 / dl));
-    s[1] = sc * ((dr - ds1) * (r1 / dr) + (dl - ds1) * (l1 / dl));
-    s[2] = sc * ((dr - ds1) * (r2 / dr) + (dl - ds1) * (l2 / dl));
-  }
-  /* stretching across fibers (column), lbm_ib.c:1233-1278 */
-  if (r == 0) {
-    const double* p = P(1, c);
-    const double t0 = p[0] - m[0], t1 = p[1] - m[1], t2 = p[2] - m[2];
-    const double dt = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
-    s[0] = s[0] + sc2 * ((dt - ds2) * (t0 / dt));
-    s[1] = s[1] + sc2 * ((dt - ds2) * (t1 / dt));
-    s[2] = s[2] + sc2 * ((dt - ds2) * (t2 / dt));
-  } else if (r == R - 1) {
-    const double* q = P(R - 2, c);
-    const double t0 = m[0] - q[0], t1 = m[1] - q[1], t2 = m[2] - q[2];
-    const double db = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
-    s[0] = s[0] + sc2 * ((db - ds2) * (t0 / db));
-    s[1] = s[1] + sc2 * ((db - ds2) * (t1 / db));
-    s[2] = s[2] + sc2 * ((db - ds2) * (t2 / db));
-  } else {
-    const double* p = P(r + 1, c);
-    const double* q = P(r - 1, c);
-    const double a0 = p[0] - m[0], a1 = p[1] - m[1], a2 = p[2] - m[2];
-    const double e0 = q[0] - m[0], e1 = q[1] - m[1], e2 = q[2] - m[2];
-    const double dt = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
-    const double db = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
-    s[0] = s[0] + sc2 * ((dt - ds2) * (a0 / dt) + (db - ds2) * (e0 / db));
-    s[1] = s[1] + sc2 * ((dt - ds2) * (a1 / dt) + (db - ds2) * (e1 / db));
-    s[2] = s[2] + sc2 * ((dt - ds2) * (a2 / dt) + (db - ds2) * (e2 / db));
-  }
-#undef P
-  double* o = nodes + (long)i * 12;
-  o[3] = b[0]; o[4] = b[1]; o[5] = b[2];
-  o[6] = s[0]; o[7] = s[1]; o[8] = s[2];
-  /* compute_elasticforce, lbm_ib.c:1303-1308: stretch + bend */
-  o[9] = s[0] + b[0]; o[10] = s[1] + b[1]; o[11] = s[2] + b[2];
+  fiber_forces_node(nodes, R, C, bc, sc, sc2, ds1, ds2, bend_bug, i);
 }
 
-__device__ __forceinline__ int stencil_start(double p) { return (int)(floor(p / 1.0 - 2) + 1); }
-
-/* Per node: stencil start, the twelve delta-kernel factors, a count for
- * every 4^3 tile the stencil touches, and per 32-node chunk the bounding box
- * of the chunk's stencils (used only for crowded tiles). */
 __global__ void lbib_node_prep(const double* __restrict__ nodes, long S, int nx, int ny, int nz, int ntx, int nty,
                                double* __restrict__ W, int* __restrict__ st, int* __restrict__ tile_cnt,
                                int* __restrict__ chunk_box, int* err, int step) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
   int b0 = INT_MAX, b1 = INT_MIN, b2 = INT_MAX, b3 = INT_MIN, b4 = INT_MAX, b5 = INT_MIN;
-  if (i < S) {
-    const double* m = nodes + i * 12;
-    const int is = stencil_start(m[0]), js = stencil_start(m[1]), ks = stencil_start(m[2]);
-    st[i * 3 + 0] = is; st[i * 3 + 1] = js; st[i * 3 + 2] = ks;
-    const double cxk = kPi / (2.0 * 1.0);
-    double* w = W + i * 12;
-    for (int a = 0; a < 4; ++a) {
-      w[a] = 1.0e0 + lbib_cos(cxk * (1.0 * (is + a) - m[0]));
-      w[4 + a] = 1.0e0 + lbib_cos(cxk * (1.0 * (js + a) - m[1]));
-      w[8 + a] = 1.0e0 + lbib_cos(cxk * (1.0 * (ks + a) - m[2]));
-    }
-    if (is < 0 || is + 3 >= nx || js < 0 || js + 3 >= ny || ks < 0 || ks + 3 >= nz) {
-      set_error(err, -3, step);
-    } else {
-      for (int tz = ks >> 2; tz <= (ks + 3) >> 2; ++tz)
-        for (int ty = js >> 2; ty <= (js + 3) >> 2; ++ty)
-          for (int tx = is >> 2; tx <= (is + 3) >> 2; ++tx) atomicAdd(&tile_cnt[((long)tz * nty + ty) * ntx + tx], 1);
-      b0 = is; b1 = is + 3; b2 = js; b3 = js + 3; b4 = ks; b5 = ks + 3;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    b0 = min(b0, __shfl_xor_sync(0xffffffffu, b0, o));
-    b1 = max(b1, __shfl_xor_sync(0xffffffffu, b1, o));
-    b2 = min(b2, __shfl_xor_sync(0xffffffffu, b2, o));
-    b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, o));
-    b4 = min(b4, __shfl_xor_sync(0xffffffffu, b4, o));
-    b5 = max(b5, __shfl_xor_sync(0xffffffffu, b5, o));
-  }
-  const long chunk = i >> 5;
-  if (lane == 0 && chunk * 32 < S) {
-    int* bx = chunk_box + chunk * 6;
-    bx[0] = b0; bx[1] = b1; bx[2] = b2; bx[3] = b3; bx[4] = b4; bx[5] = b5;
-  }
+  if (i < S) node_prep_one(nodes, i, nx, ny, nz, ntx, nty, 0, W, st, tile_cnt, err, step, b0, b1, b2, b3, b4, b5);
+  chunk_box_reduce(i, S, chunk_box, b0, b1, b2, b3, b4, b5);
 }
 
-/* Deterministic compaction of the tile counts, in tile-index order:
- * per-block sums (touched tiles, node-tile pairs), a one-block scan of both,
- * then every touched tile gets its slot and the offset of its node list. */
-constexpr int kScanBlock = 1024;
-
-__global__ void lbib_compact_count(const int* __restrict__ cnt, long n, int* __restrict__ block_tiles,
-                                   int* __restrict__ block_pairs) {
-  __shared__ int s[2][32];
-  const long i = (long)blockIdx.x * kScanBlock + threadIdx.x;
-  const int c = (i < n) ? cnt[i] : 0;
-  int v = c > 0, w = c;
-  for (int o = 16; o > 0; o >>= 1) {
-    v += __shfl_xor_sync(0xffffffffu, v, o);
-    w += __shfl_xor_sync(0xffffffffu, w, o);
-  }
-  if ((threadIdx.x & 31) == 0) { s[0][threadIdx.x >> 5] = v; s[1][threadIdx.x >> 5] = w; }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    int a = s[0][threadIdx.x], b = s[1][threadIdx.x];
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      b += __shfl_xor_sync(0xffffffffu, b, o);
-    }
-    if (threadIdx.x == 0) { block_tiles[blockIdx.x] = a; block_pairs[blockIdx.x] = b; }
-  }
-}
-
-__device__ void block_exclusive_scan(int* __restrict__ a, int n, int* total) {
-  __shared__ int s[kScanBlock];
-  int carry = 0;
-  for (int base = 0; base < n; base += kScanBlock) {
-    const int i = base + threadIdx.x;
-    const int v = (i < n) ? a[i] : 0;
-    s[threadIdx.x] = v;
-    __syncthreads();
-    for (int o = 1; o < kScanBlock; o <<= 1) {
-      const int t = (threadIdx.x >= (unsigned)o) ? s[threadIdx.x - o] : 0;
-      __syncthreads();
-      s[threadIdx.x] += t;
-      __syncthreads();
-    }
-    if (i < n) a[i] = carry + s[threadIdx.x] - v;
-    const int last = s[kScanBlock - 1];
-    __syncthreads();
-    carry += last;
-  }
-  if (threadIdx.x == 0 && total) *total = carry;
-}
-
-__global__ void lbib_compact_scan(int* __restrict__ block_tiles, int* __restrict__ block_pairs, int nblocks,
-                                  int* __restrict__ total_tiles) {
-  block_exclusive_scan(block_tiles, nblocks, total_tiles);
-  __syncthreads();
-  block_exclusive_scan(block_pairs, nblocks, nullptr);
-}
-
-__global__ void lbib_compact_write(const int* __restrict__ cnt, long n, const int* __restrict__ block_tiles,
-                                   const int* __restrict__ block_pairs, int* __restrict__ list,
-                                   int* __restrict__ slot, int* __restrict__ slot_off, int* __restrict__ slot_len,
-                                   int* __restrict__ slot_cursor) {
-  __shared__ int sv[32], sw[32];
-  const long i = (long)blockIdx.x * kScanBlock + threadIdx.x;
-  const int c = (i < n) ? cnt[i] : 0;
-  const int v = c > 0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int iv = v, iw = c;  /* inclusive warp scans */
-  for (int o = 1; o < 32; o <<= 1) {
-    const int tv = __shfl_up_sync(0xffffffffu, iv, o);
-    const int tw = __shfl_up_sync(0xffffffffu, iw, o);
-    if (lane >= o) { iv += tv; iw += tw; }
-  }
-  if (lane == 31) { sv[warp] = iv; sw[warp] = iw; }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const int a = sv[threadIdx.x], b = sw[threadIdx.x];
-    int ia = a, ib = b;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int ta = __shfl_up_sync(0xffffffffu, ia, o);
-      const int tb = __shfl_up_sync(0xffffffffu, ib, o);
-      if (lane >= o) { ia += ta; ib += tb; }
-    }
-    sv[threadIdx.x] = ia - a;
-    sw[threadIdx.x] = ib - b;
-  }
-  __syncthreads();
-  if (v) {
-    const int pos = block_tiles[blockIdx.x] + sv[warp] + iv - v;
-    list[pos] = (int)i;
-    slot[i] = pos;
-    slot_off[pos] = block_pairs[blockIdx.x] + sw[warp] + iw - c;
-    slot_len[pos] = c;
-    slot_cursor[pos] = 0;
-  }
-}
-
-/* Every node appends its index to the list of each tile its stencil touches
- * (order within a list is fixed afterwards by sorting). */
 __global__ void lbib_pair_scatter(const int* __restrict__ st, long S, int ntx, int nty, int nx, int ny, int nz,
                                   const int* __restrict__ slot, const int* __restrict__ slot_off,
-                                  int* __restrict__ slot_cursor, int* __restrict__ pair_node,
-                                  const int* err) {
+                                  int* __restrict__ slot_cursor, int* __restrict__ pair_node, const int* err) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S || *(volatile const int*)err) return;
-  const int is = st[i * 3 + 0], js = st[i * 3 + 1], ks = st[i * 3 + 2];
-  if (is < 0 || is + 3 >= nx || js < 0 || js + 3 >= ny || ks < 0 || ks + 3 >= nz) return;
-  for (int tz = ks >> 2; tz <= (ks + 3) >> 2; ++tz)
-    for (int ty = js >> 2; ty <= (js + 3) >> 2; ++ty)
-      for (int tx = is >> 2; tx <= (is + 3) >> 2; ++tx) {
-        const int s = slot[((long)tz * nty + ty) * ntx + tx];
-        const int k = atomicAdd(&slot_cursor[s], 1);
-        pair_node[slot_off[s] + k] = (int)i;
-      }
+  pair_scatter_one(st, i, ntx, nty, nx, ny, nz, slot, slot_off, slot_cursor, pair_node);
 }
 
-/* Longest per-tile node list sorted in shared memory; longer lists take the
- * chunk-scan path below. */
-constexpr int kListCap = 1024;
-
-/* One CTA (64 threads = one 4^3 tile) per touched tile: sort the tile's node
- * list by node index, then every cell adds the contributions of the nodes
- * whose stencil contains it in that order -- the reference's order. */
 __global__ void __launch_bounds__(64) lbib_spread_gather(const double* __restrict__ nodes, const double* __restrict__ W,
                                                          const int* __restrict__ st, const int* __restrict__ list,
                                                          const int* __restrict__ count, const int* __restrict__ slot_off,
                                                          const int* __restrict__ slot_len, const int* __restrict__ pair_node,
                                                          int ntx, int nty, double* __restrict__ Ftile, const int* err) {
-  __shared__ int ids[kListCap];
-  __shared__ int s_st[64][3];
-  __shared__ double s_w[64][12];
-  __shared__ double s_fe[64][3];
+  __shared__ GatherSmem sm;
   if (*(volatile const int*)err) return;
   const int n = *count;
-  const int t = threadIdx.x;
-  const double cf = 1.0 / (64.0 * 1.0 * 1.0 * 1.0);
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int L = slot_len[it];
-    if (L > kListCap) continue;
-    int P = 1;
-    while (P < L) P <<= 1;
-    const int* src = pair_node + slot_off[it];
-    __syncthreads();
-    for (int k = t; k < P; k += 64) ids[k] = (k < L) ? src[k] : INT_MAX;
-    __syncthreads();
-    for (int k = 2; k <= P; k <<= 1)
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int a = t; a < P; a += 64) {
-          const int b = a ^ j;
-          if (b > a) {
-            const int va = ids[a], vb = ids[b];
-            const bool up = (a & k) == 0;
-            if ((va > vb) == up) { ids[a] = vb; ids[b] = va; }
-          }
-        }
-        __syncthreads();
-      }
-    const int tile = list[it];
-    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
-    const int gx = tx * 4 + (t & 3), gy = ty * 4 + ((t >> 2) & 3), gz = tz * 4 + (t >> 4);
-    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-    for (int b0 = 0; b0 < L; b0 += 64) {
-      const int nb = min(64, L - b0);
-      if (t < nb) {
-        const long nd = ids[b0 + t];
-        s_st[t][0] = st[nd * 3 + 0]; s_st[t][1] = st[nd * 3 + 1]; s_st[t][2] = st[nd * 3 + 2];
-        for (int a = 0; a < 12; ++a) s_w[t][a] = W[nd * 12 + a];
-        s_fe[t][0] = nodes[nd * 12 + 9]; s_fe[t][1] = nodes[nd * 12 + 10]; s_fe[t][2] = nodes[nd * 12 + 11];
-      }
-      __syncthreads();
-      for (int j = 0; j < nb; ++j) {
-        const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
-        if ((unsigned)a < 4u && (unsigned)b < 4u && (unsigned)e < 4u) {
-          const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
-          Fx = Fx + s_fe[j][0] * tmp;
-          Fy = Fy + s_fe[j][1] * tmp;
-          Fz = Fz + s_fe[j][2] * tmp;
-        }
-      }
-      __syncthreads();
-    }
-    double* Ft = Ftile + (long)it * 192;
-    Ft[t] = Fx; Ft[64 + t] = Fy; Ft[128 + t] = Fz;
-  }
+  for (int it = blockIdx.x; it < n; it += gridDim.x)
+    gather_tile(sm, nodes, W, st, it, list[it], slot_off, slot_len, pair_node, ntx, nty, Ftile);
 }
 
-/* Crowded tiles (more than kListCap nodes, e.g. a crumpled sheet): visit the
- * nodes chunk by chunk in global order, skipping chunks whose stencil box
- * misses the tile.  Same summation order, no list needed. */
 __global__ void __launch_bounds__(64) lbib_spread_gather_scan(const double* __restrict__ nodes, const double* __restrict__ W,
                                                               const int* __restrict__ st, const int* __restrict__ chunk_box,
                                                               long S, long nchunks, const int* __restrict__ list,
                                                               const int* __restrict__ count, const int* __restrict__ slot_len,
                                                               int ntx, int nty, double* __restrict__ Ftile, const int* err) {
-  __shared__ int hit[64];
-  __shared__ int s_st[32][3];
-  __shared__ double s_w[32][12];
-  __shared__ double s_fe[32][3];
+  __shared__ ScanSmem sm;
   if (*(volatile const int*)err) return;
   const int n = *count;
-  const int cell = threadIdx.x;
-  const double cf = 1.0 / (64.0 * 1.0 * 1.0 * 1.0);
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
     if (slot_len[it] <= kListCap) continue;
-    const int tile = list[it];
-    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
-    const int x0 = tx * 4, y0 = ty * 4, z0 = tz * 4;
-    const int gx = x0 + (cell & 3), gy = y0 + ((cell >> 2) & 3), gz = z0 + (cell >> 4);
-    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-    for (long c0 = 0; c0 < nchunks; c0 += 64) {
-      const long c = c0 + cell;
-      int h = 0;
-      if (c < nchunks) {
-        const int* bx = chunk_box + c * 6;
-        h = !(bx[1] < x0 || bx[0] > x0 + 3 || bx[3] < y0 || bx[2] > y0 + 3 || bx[5] < z0 || bx[4] > z0 + 3);
-      }
-      __syncthreads();
-      hit[cell] = h;
-      __syncthreads();
-      for (int k = 0; k < 64; ++k) {
-        if (!hit[k]) continue;
-        const long base = (c0 + k) * 32;
-        if (cell < 32) {
-          const long nd = base + cell;
-          if (nd < S) {
-            s_st[cell][0] = st[nd * 3 + 0]; s_st[cell][1] = st[nd * 3 + 1]; s_st[cell][2] = st[nd * 3 + 2];
-            for (int a = 0; a < 12; ++a) s_w[cell][a] = W[nd * 12 + a];
-            s_fe[cell][0] = nodes[nd * 12 + 9]; s_fe[cell][1] = nodes[nd * 12 + 10]; s_fe[cell][2] = nodes[nd * 12 + 11];
-          } else {
-            s_st[cell][0] = INT_MIN / 2; s_st[cell][1] = INT_MIN / 2; s_st[cell][2] = INT_MIN / 2;
-          }
-        }
-        __syncthreads();
-        for (int j = 0; j < 32; ++j) {
-          const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
-          if ((unsigned)a < 4u && (unsigned)b < 4u && (unsigned)e < 4u) {
-            const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
-            Fx = Fx + s_fe[j][0] * tmp;
-            Fy = Fy + s_fe[j][1] * tmp;
-            Fz = Fz + s_fe[j][2] * tmp;
-          }
-        }
-        __syncthreads();
-      }
-    }
-    double* Ft = Ftile + (long)it * 192;
-    Ft[cell] = Fx; Ft[64 + cell] = Fy; Ft[128 + cell] = Fz;
+    gather_tile_scan(sm, nodes, W, st, chunk_box, S, 0, nchunks, it, list[it], ntx, nty, Ftile);
   }
 }
 
@@ -438,30 +67,7 @@ __global__ void lbib_move_nodes(double* __restrict__ nodes, const double* __rest
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S) return;
   if (*(volatile const int*)err) return;
-  const double c_64 = 1.0 / (6.4e1);
-  const int is = st[i * 3 + 0], js = st[i * 3 + 1], ks = st[i * 3 + 2];
-  const double* w = W + i * 12;
-  double s1 = 0, s2 = 0, s3 = 0;
-  for (int i2 = 0; i2 <= 3; i2++) {
-    const int gi = is + i2;
-    for (int j2 = 0; j2 <= 3; j2++) {
-      const int gj = js + j2;
-      for (int k2 = 0; k2 <= 3; k2++) {
-        const int gk = ks + k2;
-        const int sp = slot[lbib::tile_of(gi, gj, gk, ntx, nty)];
-        const double* U = Utile + (long)sp * 256;
-        const int cell = lbib::cell_in_tile(gi, gj, gk);
-        const double vx = U[64 + cell], vy = U[128 + cell], vz = U[192 + cell];
-        s1 += vx * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
-        s2 += vy * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
-        s3 += vz * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
-      }
-    }
-  }
-  double* m = nodes + i * 12;
-  m[0] += dt * s1;
-  m[1] += dt * s2;
-  m[2] += dt * s3;
+  move_node(nodes, W, st, i, ntx, nty, slot, Utile, dt);
 }
 
 /* Dense copy of the spread force for getters: zero, then each touched tile. */

@@ -52,6 +52,10 @@ EXPORTED = [
     "lbib_device_count", "lbib_kernel_launches", "lbib_profile_begin", "lbib_profile_end",
     "lbib_set_precision", "lbib_case_create_prec", "lbib_spread_force_noalloc", "lbib_conservation_sums",
     "lbib_kernel_variants", "lbib_set_kernel_variant", "lbib_autotune",
+    "lbib_batch_create", "lbib_batch_last_error", "lbib_batch_free", "lbib_batch_run", "lbib_batch_synchronize",
+    "lbib_batch_stream", "lbib_batch_cells", "lbib_batch_steps", "lbib_batch_kernel_launches", "lbib_batch_status",
+    "lbib_batch_get_sheet", "lbib_batch_get_moments", "lbib_batch_get_df1", "lbib_batch_variants",
+    "lbib_batch_set_variant", "lbib_batch_autotune",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -121,6 +125,25 @@ def load() -> C.CDLL:
     lib.lbib_sync_to_host.argtypes = [C.c_void_p]
     lib.do_thread.argtypes = [C.c_void_p]
     lib.do_thread.restype = C.c_void_p
+    lib.lbib_batch_create.restype = C.c_void_p
+    lib.lbib_batch_create.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int]
+    lib.lbib_batch_free.argtypes = [C.c_void_p]
+    lib.lbib_batch_free.restype = None
+    for n in ["lbib_batch_run"]:
+        getattr(lib, n).argtypes = [C.c_void_p, C.c_int]
+    for n in ["lbib_batch_synchronize", "lbib_batch_variants"]:
+        getattr(lib, n).argtypes = [C.c_void_p]
+    for n in ["lbib_batch_cells", "lbib_batch_steps", "lbib_batch_kernel_launches"]:
+        getattr(lib, n).argtypes = [C.c_void_p]
+        getattr(lib, n).restype = C.c_long
+    lib.lbib_batch_stream.argtypes = [C.c_void_p]
+    lib.lbib_batch_stream.restype = C.c_void_p
+    lib.lbib_batch_status.argtypes = [C.c_void_p, _ip, _ip]
+    lib.lbib_batch_get_sheet.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.lbib_batch_get_moments.argtypes = [C.c_void_p, C.c_int] + [_dp] * 4
+    lib.lbib_batch_get_df1.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.lbib_batch_set_variant.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.lbib_batch_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _ip]
     _lib = lib
     return lib
 
@@ -264,3 +287,120 @@ class Solver:
     def set_sheet(self, k: int, a: np.ndarray) -> None:
         a = np.ascontiguousarray(a, dtype=np.float64).ravel()
         _check(self.lib.lbib_set_sheet(self.gv, k, _ptr(a)), "lbib_set_sheet")
+
+
+class Problem(C.Structure):
+    """One problem of a batch (lbib_problem)."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("tau", C.c_double), ("u_l", C.c_double), ("Ks_l", C.c_double), ("Kb_l", C.c_double),
+                ("rows", C.c_int), ("cols", C.c_int),
+                ("width", C.c_double), ("height", C.c_double), ("x0", C.c_double), ("y0", C.c_double),
+                ("z0", C.c_double)]
+
+    @classmethod
+    def from_case(cls, case):
+        """From a one-sheet case object (the Solver's ``case``)."""
+        s = case.sheets[0]
+        return cls(case.nx, case.ny, case.nz, case.tau, case.u_l, case.Ks_l, case.Kb_l,
+                   s.rows, s.cols, s.width, s.height, s.x0, s.y0, s.z0)
+
+
+class Batch:
+    """Many independent one-sheet problems advanced together on the GPU
+    (lbib_batch_*): one launch per stage for the whole batch, the step
+    replayed as a CUDA graph."""
+
+    def __init__(self, problems, precision: str = "f64", compat: int = COMPAT_ALL):
+        lib = load()
+        self.lib = lib
+        if precision not in PRECISIONS:
+            raise LbibError(f"unknown precision {precision!r}")
+        self.problems = [p if isinstance(p, Problem) else Problem.from_case(p) for p in problems]
+        arr = (Problem * len(self.problems))(*self.problems)
+        self.h = lib.lbib_batch_create(len(self.problems), C.cast(arr, C.c_void_p), PRECISIONS[precision], compat)
+        if not self.h:
+            rc = lib.lbib_batch_last_error()
+            raise LbibError(f"lbib_batch_create failed: {lib.lbib_error_string(rc).decode()} ({rc})")
+        self.precision = precision
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.lbib_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __len__(self):
+        return len(self.problems)
+
+    def run(self, nsteps: int) -> None:
+        _check(self.lib.lbib_batch_run(self.h, nsteps), "lbib_batch_run")
+
+    def synchronize(self) -> None:
+        _check(self.lib.lbib_batch_synchronize(self.h), "lbib_batch_synchronize")
+
+    @property
+    def stream(self) -> int:
+        return self.lib.lbib_batch_stream(self.h) or 0
+
+    @property
+    def cells(self) -> int:
+        return self.lib.lbib_batch_cells(self.h)
+
+    @property
+    def steps(self) -> int:
+        return self.lib.lbib_batch_steps(self.h)
+
+    @property
+    def kernel_launches(self) -> int:
+        return self.lib.lbib_batch_kernel_launches(self.h)
+
+    def status(self):
+        """(codes, failed_step) per problem: 0 or LBIB_E_STENCIL (-3)."""
+        n = len(self.problems)
+        codes, steps = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32)
+        rc = self.lib.lbib_batch_status(self.h, codes.ctypes.data_as(_ip), steps.ctypes.data_as(_ip))
+        _check(min(rc, 0), "lbib_batch_status")
+        return codes, steps
+
+    def sheet(self, k: int) -> np.ndarray:
+        p = self.problems[k]
+        a = np.empty(p.rows * p.cols * 12)
+        _check(self.lib.lbib_batch_get_sheet(self.h, k, _ptr(a)), "lbib_batch_get_sheet")
+        return a.reshape(p.rows, p.cols, 12)
+
+    def moments(self, k: int):
+        p = self.problems[k]
+        n = p.nx * p.ny * p.nz
+        a = [np.empty(n) for _ in range(4)]
+        _check(self.lib.lbib_batch_get_moments(self.h, k, *[_ptr(x) for x in a]), "lbib_batch_get_moments")
+        return [x.reshape(p.nz, p.ny, p.nx) for x in a]
+
+    def df1(self, k: int) -> np.ndarray:
+        p = self.problems[k]
+        a = np.empty(19 * p.nx * p.ny * p.nz)
+        _check(self.lib.lbib_batch_get_df1(self.h, k, _ptr(a)), "lbib_batch_get_df1")
+        return a.reshape(19, p.nz, p.ny, p.nx)
+
+    def variants(self) -> int:
+        return self.lib.lbib_batch_variants(self.h)
+
+    def set_variant(self, v: int, k: int = -1) -> None:
+        _check(self.lib.lbib_batch_set_variant(self.h, k, v), "lbib_batch_set_variant")
+
+    def autotune(self, steps: int = 6):
+        """Pick a word-kernel variant per size class; returns (class of each
+        problem, ms per step [class][variant])."""
+        nv = self.variants()
+        cls = np.zeros(len(self.problems), dtype=np.int32)
+        ms = np.zeros(len(self.problems) * nv)
+        n = self.lib.lbib_batch_autotune(self.h, steps, _ptr(ms), len(ms), cls.ctypes.data_as(_ip))
+        _check(min(n, 0), "lbib_batch_autotune")
+        return cls, ms[: n * nv].reshape(n, nv)

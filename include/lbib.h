@@ -367,6 +367,49 @@ int lbib_stage(GV gv, int which);
 int lbib_spread_force_noalloc(const double* nodes, long num_nodes, int nx, int ny, int nz,
                               double* fx, double* fy, double* fz, void* stream);
 
+/* ---- batches of independent problems (no counterpart in the reference,
+ * which runs one problem per process) ------------------------------------
+ *
+ * Many problems of uneven size, each with its own lattice, physics and one
+ * fiber sheet, advanced together: one launch per stage for the whole batch,
+ * the step captured as a CUDA graph and replayed.  Each problem follows the
+ * same rules and arithmetic as the GV path (an FP64 batch gives every
+ * problem the bits it gets on its own); set-up mirrors init_gv_constant +
+ * gen_fluid_grid + gen_fiber_sheet + init_gv + the three init_* calls with
+ * the problem's tau, u_l, Ks_l, Kb_l.  A problem whose sheet leaves its grid
+ * stops (lbib_batch_status reports LBIB_E_STENCIL and the step); the others
+ * continue.  Sizes must be multiples of 4 (cube_size 4). */
+typedef struct lbib_problem {
+  int nx, ny, nz;                  /* lattice, x = flow direction            */
+  double tau, u_l, Ks_l, Kb_l;
+  int rows, cols;                  /* the sheet, as Fibersheet               */
+  double width, height, x0, y0, z0;
+} lbib_problem;
+typedef struct lbib_batch lbib_batch;
+
+lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision, int compat);
+int lbib_batch_last_error(void);                /* why lbib_batch_create failed */
+void lbib_batch_free(lbib_batch* b);
+int lbib_batch_run(lbib_batch* b, int nsteps);  /* asynchronous on the batch's stream */
+int lbib_batch_synchronize(lbib_batch* b);
+void* lbib_batch_stream(lbib_batch* b);
+long lbib_batch_cells(lbib_batch* b);           /* lattice sites of all problems */
+long lbib_batch_steps(lbib_batch* b);
+long lbib_batch_kernel_launches(lbib_batch* b);
+/* codes[k] = 0 or LBIB_E_STENCIL, failed_step[k] = the step it stopped at
+ * (either may be NULL); returns the number of stopped problems. */
+int lbib_batch_status(lbib_batch* b, int* codes, int* failed_step);
+int lbib_batch_get_sheet(lbib_batch* b, int k, double* out);      /* rows*cols*12 */
+int lbib_batch_get_moments(lbib_batch* b, int k, double* rho, double* ux, double* uy, double* uz);
+int lbib_batch_get_df1(lbib_batch* b, int k, double* out);
+/* Fluid word-kernel variants, set for one problem (k >= 0) or all (k = -1)
+ * before the first step, or chosen per size class by timing them;
+ * lbib_batch_autotune restores the initial state and returns the number of
+ * classes (class_of[k], ms[class * variants + v] when non-NULL). */
+int lbib_batch_variants(lbib_batch* b);
+int lbib_batch_set_variant(lbib_batch* b, int k, int variant);
+int lbib_batch_autotune(lbib_batch* b, int steps, double* ms, int max_ms, int* class_of);
+
 #ifdef __cplusplus
 }
 #endif

@@ -98,3 +98,18 @@ def test_precision_arguments_checked_before_any_gpu_call(lbib_built):
     assert lbib.PRECISIONS["f64"] == 0 and lbib.PRECISIONS["f16-flow"] == 18
     with pytest.raises(lbib.LbibError):
         lbib.Solver(small_case(), precision="f8")
+
+
+def test_batch_arguments_checked_before_any_gpu_call(lbib_built):
+    lib = lbib.load()
+    good = lbib.Problem(32, 16, 16, 0.6, 0.01, 0.05, 0.005, 4, 4, 1.5, 1.5, 10.0, 7.0, 7.0)
+    for bad in [lbib.Problem(30, 16, 16, 0.6, 0.01, 0.05, 0.005, 4, 4, 1.5, 1.5, 10.0, 7.0, 7.0),   # not /4
+                lbib.Problem(32, 16, 16, 0.5, 0.01, 0.05, 0.005, 4, 4, 1.5, 1.5, 10.0, 7.0, 7.0),   # tau
+                lbib.Problem(32, 16, 16, 0.6, 0.01, 0.05, 0.005, 1, 4, 1.5, 1.5, 10.0, 7.0, 7.0)]:  # rows
+        arr = (lbib.Problem * 2)(good, bad)
+        assert not lib.lbib_batch_create(2, ctypes.cast(arr, ctypes.c_void_p), 0, 7)
+        assert lib.lbib_batch_last_error() == -1
+    arr = (lbib.Problem * 1)(good)
+    for prec in (-1, 4, 16):
+        assert not lib.lbib_batch_create(1, ctypes.cast(arr, ctypes.c_void_p), prec, 7)
+    assert not lib.lbib_batch_create(0, None, 0, 7)
