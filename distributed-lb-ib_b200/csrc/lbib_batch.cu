@@ -53,10 +53,14 @@ __global__ void lbib_b_forces(double* __restrict__ nodes, const int* __restrict_
                     (int)(i - d.node0));
 }
 
+/* step_no: the batch's device step counter (graph replays see the live
+ * value), 1 for the first step. */
 __global__ void lbib_b_node_prep(const double* __restrict__ nodes, const int* __restrict__ node_inst,
                                  const BatchDesc* __restrict__ D, double* __restrict__ W, int* __restrict__ st,
-                                 int* __restrict__ tile_cnt, int* __restrict__ chunk_box, int* err, long SP, int step) {
+                                 int* __restrict__ tile_cnt, int* __restrict__ chunk_box, int* err, long SP,
+                                 const int* __restrict__ step_no) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int step = *step_no;
   int b0 = INT_MAX, b1 = INT_MIN, b2 = INT_MAX, b3 = INT_MIN, b4 = INT_MAX, b5 = INT_MIN;
   const int k = i < SP ? node_inst[i] : -1;
   if (k >= 0 && !err[2 * k]) {
@@ -119,12 +123,15 @@ __global__ void __launch_bounds__(64) lbib_b_gather_scan(const double* __restric
 
 __global__ void lbib_b_move(double* __restrict__ nodes, const double* __restrict__ W, const int* __restrict__ st,
                             const int* __restrict__ node_inst, const BatchDesc* __restrict__ D,
-                            const int* __restrict__ slot, const double* __restrict__ Utile, const int* err, long SP) {
+                            const int* __restrict__ slot, const double* __restrict__ Utile, const int* err, long SP,
+                            int* __restrict__ step_no) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) ++*step_no;   /* the last kernel of the step; node_prep has read it */
   if (i >= SP) return;
   const int k = node_inst[i];
   if (k < 0 || *(volatile const int*)(err + 2 * k)) return;
   const BatchDesc& d = D[k];
+  if (d.pinned && i - d.node0 < d.cols) return;
   move_node(nodes, W, st, i, d.ntx, d.nty, slot + d.tile0, Utile, d.dt);
 }
 
@@ -179,6 +186,7 @@ struct lbib_batch {
   double *nodes, *W;
   int *st, *node_inst, *chunk_box;
   int *err, *h_err;
+  int* step_no;                  /* device step counter, 1-based */
   long NT, CAP, SP, cells;
   /* per-problem fluid parameters: [cur] with first = 0, and the first step */
   void *P[2], *P_first, *WP[2], *WP_first;
@@ -360,7 +368,7 @@ int batch_step(lbib_batch* b) {
   CK(cudaMemsetAsync(b->tile_cnt, 0, sizeof(int) * b->NT, s));
   CK(cudaMemsetAsync(b->tile_slot[c], 0xff, sizeof(int) * b->NT, s));
   lbib_b_node_prep<<<nb, 128, 0, s>>>(b->nodes, b->node_inst, b->desc, b->W, b->st, b->tile_cnt, b->chunk_box, b->err,
-                                      SP, (int)b->steps + 1);
+                                      SP, b->step_no);
   const unsigned nblk = (unsigned)((b->NT + kScan - 1) / kScan);
   int* block_tiles = b->scan_tmp;
   int* block_pairs = b->scan_tmp + nblk + 1;
@@ -396,7 +404,7 @@ int batch_step(lbib_batch* b) {
   BatchFluid g = fluid_args(b, par ^ 1, b->P[c], b->WP[c], c);
   if ((is_lp(b) ? batch_tile_moments_lp(g) : batch_tile_moments_f64(g))) return -2;
   lbib_b_move<<<nb, 128, 0, s>>>(b->nodes, b->W, b->st, b->node_inst, b->desc, b->tile_slot[c], b->Utile[c], b->err,
-                                 SP);
+                                 SP, b->step_no);
   b->launches += 2;
   b->cur = c;
   b->parity ^= 1;
@@ -433,6 +441,9 @@ int init_state(lbib_batch* b) {
   }
   CK(cudaMemsetAsync(b->tile_slot[0], 0xff, sizeof(int) * b->NT, b->stream));
   CK(cudaMemsetAsync(b->tile_slot[1], 0xff, sizeof(int) * b->NT, b->stream));
+  const int one = 1;
+  CK(cudaMemcpyAsync(b->step_no, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
   b->steps = 0;
   b->parity = 0;
   b->cur = 0;
@@ -498,6 +509,7 @@ lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision
     BatchDesc& D = b->h_desc[k];
     D.nx = p->nx; D.ny = p->ny; D.nz = p->nz; D.ntx = d->ntx; D.nty = d->nty;
     D.rows = p->rows; D.cols = p->cols;
+    D.pinned = p->pinned != 0;
     D.tile0 = tile0; D.ntiles = d->ntiles;
     D.node0 = node0; D.S = (long)p->rows * p->cols;
     D.ds1 = p->width / (p->cols - 1);
@@ -554,6 +566,7 @@ lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision
   if (!rc && cudaMalloc(&b->chunk_box, sizeof(int) * 6 * (SP / 32 + 1)) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&b->err, sizeof(int) * 2 * n) != cudaSuccess) rc = -5;
   if (!rc && cudaMallocHost(&b->h_err, sizeof(int) * 2 * n) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&b->step_no, sizeof(int)) != cudaSuccess) rc = -5;
   if (!rc && cudaMemset(b->err, 0, sizeof(int) * 2 * n) != cudaSuccess) rc = -2;
   if (!rc && cudaMalloc(&b->desc, sizeof(BatchDesc) * n) != cudaSuccess) rc = -5;
   if (!rc && cudaMemcpy(b->desc, b->h_desc, sizeof(BatchDesc) * n, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
@@ -661,6 +674,7 @@ void lbib_batch_free(lbib_batch* b) {
   cudaFree(b->P_first); cudaFree(b->WP_first);
   cudaFree(b->nodes); cudaFree(b->W); cudaFree(b->st); cudaFree(b->node_inst); cudaFree(b->chunk_box);
   cudaFree(b->err);
+  cudaFree(b->step_no);
   if (b->h_err) cudaFreeHost(b->h_err);
   cudaFree(b->desc); cudaFree(b->rows); cudaFree(b->edge_off);
   for (int v = 0; v < MAXV; ++v) cudaFree(b->wblk[v]);

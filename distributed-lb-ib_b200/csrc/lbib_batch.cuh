@@ -31,6 +31,7 @@ struct BatchDesc {
   int nx, ny, nz, ntx, nty;
   int rows, cols;          /* its one sheet */
   int bulk;                /* bulk rows run the word kernel */
+  int pinned;              /* row 0 of the sheet stays put */
   long tile0, ntiles;      /* slice of the global tile space */
   long node0, S;           /* nodes [node0, node0 + S); node0 % 32 == 0 */
   double bc, sc, sc2, ds1, ds2, dt;

@@ -295,14 +295,14 @@ class Problem(C.Structure):
                 ("tau", C.c_double), ("u_l", C.c_double), ("Ks_l", C.c_double), ("Kb_l", C.c_double),
                 ("rows", C.c_int), ("cols", C.c_int),
                 ("width", C.c_double), ("height", C.c_double), ("x0", C.c_double), ("y0", C.c_double),
-                ("z0", C.c_double)]
+                ("z0", C.c_double), ("pinned", C.c_int)]
 
     @classmethod
     def from_case(cls, case):
         """From a one-sheet case object (the Solver's ``case``)."""
         s = case.sheets[0]
         return cls(case.nx, case.ny, case.nz, case.tau, case.u_l, case.Ks_l, case.Kb_l,
-                   s.rows, s.cols, s.width, s.height, s.x0, s.y0, s.z0)
+                   s.rows, s.cols, s.width, s.height, s.x0, s.y0, s.z0, int(getattr(case, "pinned", 0)))
 
 
 class Batch:

@@ -384,6 +384,9 @@ typedef struct lbib_problem {
   double tau, u_l, Ks_l, Kb_l;
   int rows, cols;                  /* the sheet, as Fibersheet               */
   double width, height, x0, y0, z0;
+  int pinned;                      /* 1: row 0 of the sheet does not move (a
+                                      flap hinged at its leading edge; not in
+                                      the reference, whose sheets are free) */
 } lbib_problem;
 typedef struct lbib_batch lbib_batch;
 

@@ -102,7 +102,7 @@ def test_precision_arguments_checked_before_any_gpu_call(lbib_built):
 
 def test_batch_arguments_checked_before_any_gpu_call(lbib_built):
     lib = lbib.load()
-    good = lbib.Problem(32, 16, 16, 0.6, 0.01, 0.05, 0.005, 4, 4, 1.5, 1.5, 10.0, 7.0, 7.0)
+    good = lbib.Problem(32, 16, 16, 0.6, 0.01, 0.05, 0.005, 4, 4, 1.5, 1.5, 10.0, 7.0, 7.0, 0)
     for bad in [lbib.Problem(30, 16, 16, 0.6, 0.01, 0.05, 0.005, 4, 4, 1.5, 1.5, 10.0, 7.0, 7.0),   # not /4
                 lbib.Problem(32, 16, 16, 0.5, 0.01, 0.05, 0.005, 4, 4, 1.5, 1.5, 10.0, 7.0, 7.0),   # tau
                 lbib.Problem(32, 16, 16, 0.6, 0.01, 0.05, 0.005, 1, 4, 1.5, 1.5, 10.0, 7.0, 7.0)]:  # rows

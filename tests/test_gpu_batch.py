@@ -110,3 +110,25 @@ def test_autotune_per_size_class(gpu):
             b.set_variant(int(np.argmin(ms[cls[k]])), k)
         b.run(5)
         np.testing.assert_array_equal(b.df1(3), a)
+
+
+def test_pinned_leading_row_stays(gpu):
+    case = problems()[0]
+    p = lbib.Problem.from_case(case)
+    p.pinned = 1
+    with lbib.Batch([p, lbib.Problem.from_case(case)], "f64") as b:
+        s0 = b.sheet(0)
+        b.run(6)
+        s1, free = b.sheet(0), b.sheet(1)
+    np.testing.assert_array_equal(s1[0, :, :3], s0[0, :, :3])
+    assert np.abs(s1[1:, :, :3] - s0[1:, :, :3]).max() > 0
+    assert np.abs(free[0, :, :3] - s0[0, :, :3]).max() > 0
+
+
+def test_failure_step_counts_through_graph_replays(gpu):
+    """The step a problem stops at is the live step, also inside replayed graphs."""
+    bad = Case(32, 16, 16, [Sheet(4, 4, 1.5, 1.5, 26.0, 7.0, 7.0)], u_l=0.1)
+    with lbib.Batch([bad, problems()[0]], "f64") as b:
+        b.run(80)
+        codes, step = b.status()
+    assert codes[0] == -3 and step[0] > 6 and codes[1] == 0
