@@ -387,6 +387,9 @@ def run_lbib(args):
                          f"{sc.nx}), {sc.sheets[0].rows}x{sc.sheets[0].cols} sheet, {args.cpu_steps} steps"}
 
     solver.close()
+    sweep_leg = None
+    if args.sweep_n > 0 and args.precision == "f64":
+        sweep_leg = run_sweep_leg(args, group)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -400,10 +403,41 @@ def run_lbib(args):
                              "bytes_per_launch": bytes_launch, "launch_ms": fluid_ms},
                 "stages_ms_per_step": {k: v / max(nprof, 1) for k, v in stage_ms.items()},
                 "gpu_launches": launches, "autotune": tuned, "fp16_store": lp,
-                "e2e": e2e, "cpu_baseline": cpu, "clocks": clk}
+                "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "sweep": sweep_leg}
         print(json.dumps(line), flush=True)
     group.close()
     return 0
+
+
+def run_sweep_leg(args, group):
+    """The batched parameter sweep (sweep.py: 256 uneven problems, seed 1,
+    2000 steps, pinned flaps), once in FP16 storage and once in FP64, each as
+    one batch per GPU.  points/s = problems of all ranks / max wall time;
+    a point is within 2% when its FP16 tip displacement is within 2% of its
+    FP64 one (both runs reached the end)."""
+    import numpy as np
+
+    import sweep
+    probs = sweep.draw_problems(args.sweep_n, 1)
+    out = {}
+    for prec in ("f16-flow", "f64"):
+        group.barrier()
+        r = sweep.run_sweep(probs, args.sweep_steps, prec)
+        wall = group.max(r["wall_s"])
+        out[prec] = {"points_per_s": group.world * len(probs) / wall, "wall_s": wall,
+                     "mlups": r["mlups"], "gpu_launches": r["kernel_launches"], "stopped": r["stopped"],
+                     "autotuned_size_classes": (r["autotune"] or {}).get("classes"),
+                     "tips": r["tip_displacement"], "completed": r["completed"]}
+    t16, t64 = np.array(out["f16-flow"].pop("tips")), np.array(out["f64"].pop("tips"))
+    both = np.array(out["f16-flow"].pop("completed")) & np.array(out["f64"].pop("completed"))
+    stopped16 = out["f16-flow"]["stopped"]
+    ok = both & (np.abs(t16 - t64) <= 0.02 * np.maximum(np.abs(t64), 1e-3))
+    return {"workload": f"{len(probs)} problems (sweep.py, seed 1), {args.sweep_steps} steps, one batch per GPU",
+            "unit": "points/s", "fp16_batched": out["f16-flow"], "fp64_batched": out["f64"],
+            "speedup_fp16_vs_fp64": out["f16-flow"]["points_per_s"] / out["f64"]["points_per_s"],
+            "completed_both": int(both.sum()), "tip_within_2pct_of_fp64": int(ok.sum()), "stopped_fp16": stopped16,
+            "note": "a point whose sheet left its grid stops there and counts as run; tips are compared on "
+                    "the points both runs completed"}
 
 
 def run_lp_form(args, case, ref_solver, group, value64, peak):
@@ -465,6 +499,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sweep-n", type=int, default=256, help="problems of the batched sweep leg (0: skip)")
+    ap.add_argument("--sweep-steps", type=int, default=2000)
     ap.add_argument("--lp-form", default="f16-flow",
                     help="low-precision form timed beside the FP64 leg (or 'none')")
     ap.add_argument("--variant", type=int, default=None,

@@ -91,6 +91,7 @@ def run_sweep(problems, steps: int, precision: str = "f16-flow", autotune: bool 
             "points_per_s": len(problems) / wall, "wall_s": wall, "gpu_s": gpu_s, "setup_s": t_setup,
             "mlups": cells * steps / gpu_s / 1e6, "cells": cells, "kernel_launches": launches,
             "stopped": int((codes != 0).sum()), "stopped_at": [int(s) for s in failed_at[codes != 0]],
+            "completed": [bool(c == 0) for c in codes],
             "tip_displacement": tips, "autotune": tuned}
 
 
