@@ -56,6 +56,8 @@ EXPORTED = [
     "lbib_batch_stream", "lbib_batch_cells", "lbib_batch_steps", "lbib_batch_kernel_launches", "lbib_batch_status",
     "lbib_batch_get_sheet", "lbib_batch_get_moments", "lbib_batch_get_df1", "lbib_batch_variants",
     "lbib_batch_set_variant", "lbib_batch_autotune",
+    "lbib_mlp_create", "lbib_mlp_free", "lbib_mlp_param_count", "lbib_mlp_stream", "lbib_mlp_get_params",
+    "lbib_mlp_set_params", "lbib_mlp_forward", "lbib_mlp_gradient", "lbib_mlp_train_step", "lbib_mlp_synchronize",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -144,6 +146,21 @@ def load() -> C.CDLL:
     lib.lbib_batch_get_df1.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.lbib_batch_set_variant.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.lbib_batch_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _ip]
+    _fp = C.POINTER(C.c_float)
+    lib.lbib_mlp_create.restype = C.c_void_p
+    lib.lbib_mlp_create.argtypes = [C.c_int, _ip, C.c_int, C.c_ulonglong]
+    lib.lbib_mlp_free.argtypes = [C.c_void_p]
+    lib.lbib_mlp_free.restype = None
+    lib.lbib_mlp_param_count.argtypes = [C.c_void_p]
+    lib.lbib_mlp_param_count.restype = C.c_long
+    lib.lbib_mlp_stream.argtypes = [C.c_void_p]
+    lib.lbib_mlp_stream.restype = C.c_void_p
+    lib.lbib_mlp_get_params.argtypes = [C.c_void_p, _fp]
+    lib.lbib_mlp_set_params.argtypes = [C.c_void_p, _fp]
+    lib.lbib_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    lib.lbib_mlp_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, _fp, _fp]
+    lib.lbib_mlp_train_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, _fp]
+    lib.lbib_mlp_synchronize.argtypes = [C.c_void_p]
     _lib = lib
     return lib
 
@@ -404,3 +421,77 @@ class Batch:
         n = self.lib.lbib_batch_autotune(self.h, steps, _ptr(ms), len(ms), cls.ctypes.data_as(_ip))
         _check(min(n, 0), "lbib_batch_autotune")
         return cls, ms[: n * nv].reshape(n, nv)
+
+
+class MLP:
+    """The GPU MLP of the sweep surrogate (lbib_mlp_*).  Arrays passed to
+    forward / gradient / train_step are CUDA tensors (float32, contiguous,
+    [batch, width]); torch only provides the device memory."""
+
+    def __init__(self, widths, max_batch: int = 1024, seed: int = 0):
+        lib = load()
+        self.lib = lib
+        self.widths = list(widths)
+        w = (C.c_int * len(widths))(*widths)
+        self.h = lib.lbib_mlp_create(len(widths) - 1, w, max_batch, seed)
+        if not self.h:
+            raise LbibError("lbib_mlp_create failed")
+        self.max_batch = max_batch
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.lbib_mlp_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def nparams(self) -> int:
+        return self.lib.lbib_mlp_param_count(self.h)
+
+    def params(self) -> np.ndarray:
+        a = np.empty(self.nparams, dtype=np.float32)
+        _check(self.lib.lbib_mlp_get_params(self.h, a.ctypes.data_as(C.POINTER(C.c_float))), "lbib_mlp_get_params")
+        return a
+
+    def set_params(self, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        assert a.size == self.nparams
+        _check(self.lib.lbib_mlp_set_params(self.h, a.ctypes.data_as(C.POINTER(C.c_float))), "lbib_mlp_set_params")
+
+    @staticmethod
+    def _dev(t, width):
+        assert t.is_cuda and t.dtype.is_floating_point and t.is_contiguous() and t.shape[-1] == width
+        return C.c_void_p(t.data_ptr())
+
+    def forward(self, X):
+        import torch
+        Y = torch.empty((X.shape[0], self.widths[-1]), dtype=torch.float32, device=X.device)
+        _check(self.lib.lbib_mlp_forward(self.h, self._dev(X, self.widths[0]), X.shape[0], self._dev(Y, self.widths[-1])),
+               "lbib_mlp_forward")
+        return Y
+
+    def gradient(self, X, T):
+        g = np.empty(self.nparams, dtype=np.float32)
+        loss = C.c_float(0.0)
+        _check(self.lib.lbib_mlp_gradient(self.h, self._dev(X, self.widths[0]), self._dev(T, self.widths[-1]),
+                                          X.shape[0], g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)),
+               "lbib_mlp_gradient")
+        return g, loss.value
+
+    def train_step(self, X, T, lr: float, want_loss: bool = False):
+        loss = C.c_float(0.0)
+        _check(self.lib.lbib_mlp_train_step(self.h, self._dev(X, self.widths[0]), self._dev(T, self.widths[-1]),
+                                            X.shape[0], lr, C.byref(loss) if want_loss else None),
+               "lbib_mlp_train_step")
+        return loss.value if want_loss else None
+
+    def synchronize(self) -> None:
+        _check(self.lib.lbib_mlp_synchronize(self.h), "lbib_mlp_synchronize")

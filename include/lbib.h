@@ -413,6 +413,28 @@ int lbib_batch_variants(lbib_batch* b);
 int lbib_batch_set_variant(lbib_batch* b, int k, int variant);
 int lbib_batch_autotune(lbib_batch* b, int steps, double* ms, int max_ms, int* class_of);
 
+/* ---- a small MLP trained on the GPU: the sweep surrogate (no counterpart
+ * in the reference) ------------------------------------------------------
+ *
+ * widths[0..n_layers]: input, hidden..., output; GELU after every layer but
+ * the last; BF16 weights and activations with FP32 accumulation on the
+ * tensor cores; FP32 master weights; mean-squared-error loss; Adam (beta1
+ * 0.9, beta2 0.999, eps 1e-8).  Parameters, in order: per layer W
+ * [out][in] row-major, then b [out].  X, T, Y of forward/train/gradient are
+ * device pointers to row-major FP32 [batch][width] arrays; grad and loss of
+ * lbib_mlp_gradient are host memory.  Returns NULL / error codes as above. */
+typedef struct lbib_mlp lbib_mlp;
+lbib_mlp* lbib_mlp_create(int n_layers, const int* widths, int max_batch, unsigned long long seed);
+void lbib_mlp_free(lbib_mlp* n);
+long lbib_mlp_param_count(lbib_mlp* n);
+void* lbib_mlp_stream(lbib_mlp* n);
+int lbib_mlp_get_params(lbib_mlp* n, float* out);
+int lbib_mlp_set_params(lbib_mlp* n, const float* in);
+int lbib_mlp_forward(lbib_mlp* n, const float* X, int batch, float* Y);
+int lbib_mlp_gradient(lbib_mlp* n, const float* X, const float* T, int batch, float* grad, float* loss);
+int lbib_mlp_train_step(lbib_mlp* n, const float* X, const float* T, int batch, float lr, float* loss);
+int lbib_mlp_synchronize(lbib_mlp* n);
+
 #ifdef __cplusplus
 }
 #endif
