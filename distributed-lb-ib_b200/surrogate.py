@@ -1,0 +1,226 @@
+"""A learned screen for parameter sweeps: an MLP surrogate trained on
+trajectories the batched solver generates, with the plain solver as its
+fallback and judge.
+
+Workload (the learned-sweep benchmark): problems on a 96 x 48 x 48 lattice
+with a 32 x 32 sheet (spacing 0.5, plane x = 16, centred, free as in the
+reference), parameters (Ks, Kb, tau, u_x) drawn as in the batched sweep
+(log-uniform Ks in [1e-3, 1e-1], Kb in [1e-4, 1e-2], tau in [0.55, 0.9],
+u_x in [0.005, 0.03]); training runs from default_rng(2), held-out sweep
+points from default_rng(3); T = 3000 steps.
+
+Model: inputs (log10 Ks, log10 Kb, tau, u_x, t/T), affinely scaled to about
+[-1, 1]; 4 hidden layers of 256 with GELU; outputs the x, y, z displacement
+of an 8 x 8 subsample of the sheet's nodes (rows and columns 0, 4, 9, 13,
+18, 22, 27, 31) since t = 0, scaled by 1/20, plus one more output: whether
+the run is still going at t (1) or has stopped because its sheet left the
+grid (0) -- many runs of this parameter range do.  Trained by the library's
+own GPU kernels (lbib_mlp_*: BF16 tensor-core GEMMs, Adam), two members with
+different seeds.
+
+Screen: both members predict every point at t = T.  A point is re-run by the
+plain FP64 solver when it is among the top 5% by predicted tip displacement
+(the points a sweep is after), when the members disagree on its tip by more
+than `disagree` (relative), or when the stop output is undecided (between
+0.2 and 0.8); every other point is reported from the surrogate.  The judge:
+the plain FP64 solver on every point, which the report compares against --
+tip displacement = mean x-displacement of the subsample's last row.
+"""
+from __future__ import annotations
+
+import time
+from typing import Dict, List
+
+import numpy as np
+
+import lbib
+import sweep
+
+NX, NY, NZ, SIDE = 96, 48, 48, 32
+SUB = np.round(np.arange(8) * (SIDE - 1) / 7.0).astype(int)  # 0 4 9 13 18 22 27 31
+DISP_SCALE = 20.0
+
+
+def draw(n: int, seed: int, pinned: bool = False) -> List[lbib.Problem]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        ks = float(10 ** rng.uniform(-3, -1))
+        kb = float(10 ** rng.uniform(-4, -2))
+        tau = float(rng.uniform(0.55, 0.9))
+        u = float(rng.uniform(0.005, 0.03))
+        out.append(sweep.make_problem(NX, NY, NZ, SIDE, ks, kb, tau, u, pinned))
+    return out
+
+
+def subsample(sheet: np.ndarray) -> np.ndarray:
+    return sheet[SUB][:, SUB, :3].reshape(64, 3)
+
+
+def simulate(problems, steps: int, every: int, precision: str, chunk: int = 1024):
+    """Run the problems in batches of `chunk`; returns the subsample
+    displacement [n, snaps, 64, 3] at t = every, 2 every, ..., steps, the
+    alive flag [n, snaps], each problem's stop step (0 = completed) and the
+    wall-clock seconds (set-up included)."""
+    n = len(problems)
+    snaps = steps // every
+    disp = np.zeros((n, snaps, 64, 3), dtype=np.float32)
+    alive = np.ones((n, snaps), dtype=bool)
+    stop = np.zeros(n, dtype=np.int64)
+    t0 = time.perf_counter()
+    for c0 in range(0, n, chunk):
+        part = problems[c0:c0 + chunk]
+        with lbib.Batch(part, precision, compat=0) as b:
+            if b.variants() > 1:
+                b.autotune(4)
+            x0 = [subsample(b.sheet(k)) for k in range(len(part))]
+            for s in range(snaps):
+                b.run(every)
+                codes, at = b.status()
+                for k in range(len(part)):
+                    disp[c0 + k, s] = subsample(b.sheet(k)) - x0[k]
+                    if codes[k]:
+                        alive[c0 + k, s] = False
+                        stop[c0 + k] = at[k]
+    return disp, alive, stop, time.perf_counter() - t0
+
+
+def features(problems, tfrac) -> np.ndarray:
+    p = np.array([[np.log10(q.Ks_l), np.log10(q.Kb_l), q.tau, q.u_l] for q in problems])
+    x = np.empty((len(problems), 5), dtype=np.float32)
+    x[:, 0] = (p[:, 0] + 2.0)          # [-1, 1]
+    x[:, 1] = (p[:, 1] + 3.0)
+    x[:, 2] = (p[:, 2] - 0.725) / 0.175
+    x[:, 3] = (p[:, 3] - 0.0175) / 0.0125
+    x[:, 4] = 2.0 * np.asarray(tfrac) - 1.0
+    return x
+
+
+def training_set(problems, disp, alive):
+    n, snaps = alive.shape
+    tf = np.repeat(((np.arange(snaps) + 1) / snaps)[None, :], n, axis=0).ravel()
+    X = features([problems[i] for i in range(n) for _ in range(snaps)], tf)
+    Y = np.concatenate([disp.reshape(n * snaps, 192) / DISP_SCALE, alive.reshape(n * snaps, 1)], axis=1)
+    return X, Y.astype(np.float32)
+
+
+WIDTHS = [5, 256, 256, 256, 256, 193]
+
+
+def train(X, Y, members: int = 2, iters: int = 4000, batch: int = 1024, lr: float = 1e-3):
+    """Train `members` nets on the GPU; returns them and the loss curves."""
+    import torch
+    Xd = torch.from_numpy(X).cuda()
+    Yd = torch.from_numpy(Y).cuda()
+    n = X.shape[0]
+    nets, curves = [], []
+    for m in range(members):
+        net = lbib.MLP(WIDTHS, max_batch=batch, seed=100 + m)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1000 + m)
+        curve = []
+        for it in range(iters):
+            idx = torch.randint(0, n, (batch,), device="cuda", generator=g)
+            xb, yb = Xd[idx].contiguous(), Yd[idx].contiguous()
+            step_lr = lr * (0.1 ** (it / iters))
+            want = it % 500 == 0 or it == iters - 1
+            loss = net.train_step(xb, yb, step_lr, want_loss=want)
+            if want:
+                curve.append((it, loss))
+        net.synchronize()
+        nets.append(net)
+        curves.append(curve)
+    return nets, curves
+
+
+def predict(nets, problems):
+    import torch
+    X = torch.from_numpy(features(problems, np.ones(len(problems)))).cuda()
+    outs = []
+    for net in nets:
+        Y = []
+        for c0 in range(0, X.shape[0], net.max_batch):
+            Y.append(net.forward(X[c0:c0 + net.max_batch].contiguous()))
+        outs.append(torch.cat(Y).cpu().numpy())
+    outs = np.stack(outs)                         # [members, n, 193]
+    disp = outs[..., :192].reshape(len(nets), len(problems), 64, 3) * DISP_SCALE
+    tip = disp[..., 56:64, 0].mean(axis=-1)       # last subsample row, x
+    alive = outs[..., 192]
+    return tip, alive
+
+
+def tip_of(disp_final: np.ndarray) -> np.ndarray:
+    return disp_final[:, 56:64, 0].mean(axis=-1)
+
+
+def screen(nets, problems, top: float = 0.05, disagree: float = 0.02):
+    """Which points the surrogate reports and which go to the plain solver."""
+    t0 = time.perf_counter()
+    tip, alive = predict(nets, problems)
+    m_tip, m_alive = tip.mean(axis=0), alive.mean(axis=0)
+    spread = np.abs(tip[0] - tip[-1]) / np.maximum(np.abs(m_tip), 1e-3)
+    rerun = spread > disagree
+    rerun |= (m_alive > 0.2) & (m_alive < 0.8)
+    k = max(1, int(round(top * len(problems))))
+    rerun[np.argsort(-np.abs(m_tip))[:k]] = True
+    return {"tip": m_tip, "alive": m_alive > 0.5, "rerun": rerun, "seconds": time.perf_counter() - t0}
+
+
+def evaluate(nets, problems, steps: int, truth=None) -> Dict:
+    """Screen `problems`, re-run the flagged ones with the plain FP64 solver,
+    and judge every reported point against the plain solver's own run."""
+    s = screen(nets, problems)
+    idx = np.nonzero(s["rerun"])[0]
+    rerun_s = 0.0
+    if len(idx):
+        d, a, _, rerun_s = simulate([problems[i] for i in idx], steps, steps, "f64")
+    if truth is None:
+        truth = simulate(problems, steps, steps, "f64")
+    tdisp, talive, _, plain_s = truth
+    true_tip = tip_of(tdisp[:, -1])
+    true_alive = talive[:, -1]
+    rep = ~s["rerun"]
+    # a reported point is right when it gets "stopped" right, and, for a run
+    # that completes, its tip within 2% (or 0.02 lattice units for tiny tips)
+    tip_ok = np.abs(s["tip"] - true_tip) <= np.maximum(0.02 * np.abs(true_tip), 0.02)
+    right = (s["alive"] == true_alive) & (~true_alive | tip_ok)
+    sur_s = s["seconds"] + rerun_s
+    return {"points": len(problems), "reported_by_surrogate": int(rep.sum()), "rerun": int(len(idx)),
+            "plain_fp64_s": plain_s, "plain_points_per_s": len(problems) / plain_s,
+            "surrogate_s": sur_s, "surrogate_points_per_s": len(problems) / sur_s,
+            "speedup": plain_s / sur_s,
+            "reported_right": int(right[rep].sum()), "reported_right_frac": float(right[rep].mean()) if rep.any() else 1.0,
+            "reported_completed": int((rep & true_alive).sum()),
+            "reported_completed_tip_within_2pct": int((rep & true_alive & tip_ok).sum()),
+            "stop_prediction_accuracy": float((s["alive"] == true_alive).mean())}
+
+
+def main(argv=None) -> int:
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="learned sweep screen")
+    ap.add_argument("--train-n", type=int, default=4096)
+    ap.add_argument("--eval-n", type=int, default=2048)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--every", type=int, default=100)
+    ap.add_argument("--iters", type=int, default=4000)
+    a = ap.parse_args(argv)
+    out = {}
+    tr = draw(a.train_n, 2)
+    disp, alive, stop, gen_s = simulate(tr, a.steps, a.every, "f16-flow")
+    out["training_runs"] = {"n": a.train_n, "seconds": gen_s, "completed": int(alive[:, -1].sum())}
+    X, Y = training_set(tr, disp, alive)
+    t0 = time.perf_counter()
+    nets, curves = train(X, Y, iters=a.iters)
+    out["training"] = {"samples": int(X.shape[0]), "seconds": time.perf_counter() - t0, "loss_curves": curves}
+    ev = draw(a.eval_n, 3)
+    out["evaluation"] = evaluate(nets, ev, a.steps)
+    for n in nets:
+        n.close()
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
