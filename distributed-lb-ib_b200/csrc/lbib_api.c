@@ -282,6 +282,69 @@ int lbib_autotune(GV gv, int steps, double* ms_per_variant, int max_variants) {
   return rc ? set_error(rc) : best;
 }
 
+/* ---- restart files ---------------------------------------------------- */
+
+/* File header: magic, layout version, the grid, precision, compat, the
+ * sheets' shapes, physics and gv->time; the GPU state follows. */
+#define LBIB_RESTART_MAGIC "LBIBRST1"
+
+int lbib_save_restart(GV gv, const char* path) {
+  if (!gv || !gv->dev || !gv->fiber_shape || !path) return set_error(LBIB_E_STATE);
+  FILE* fp = fopen(path, "wb");
+  if (!fp) return set_error(LBIB_E_IO);
+  lbib_device* d = gv->dev;
+  int h[8] = {1, d->nx, d->ny, d->nz, d->prec, d->compat, gv->fiber_shape->num_sheets, gv->time};
+  double phys[8] = {d->tau, d->u_l, d->rho_l, d->Ks_l, d->Kb_l, d->g_l, d->cs_l, (double)d->dt};
+  int ok = fwrite(LBIB_RESTART_MAGIC, 1, 8, fp) == 8 && fwrite(h, sizeof(h), 1, fp) == 1 &&
+           fwrite(phys, sizeof(phys), 1, fp) == 1;
+  for (int k = 0; ok && k < gv->fiber_shape->num_sheets; ++k) {
+    const int rc2[2] = {gv->fiber_shape->sheets[k].num_rows, gv->fiber_shape->sheets[k].num_cols};
+    ok = fwrite(rc2, sizeof(rc2), 1, fp) == 1;
+  }
+  int rc = ok ? lbdev_save_state(d, fp) : LBIB_E_IO;
+  if (fclose(fp) != 0 && !rc) rc = LBIB_E_IO;
+  return rc ? set_error(rc) : LBIB_OK;
+}
+
+int lbib_load_restart(GV gv, const char* path) {
+  if (!gv || !gv->dev || !gv->fiber_shape || !path) return set_error(LBIB_E_STATE);
+  FILE* fp = fopen(path, "rb");
+  if (!fp) return set_error(LBIB_E_IO);
+  lbib_device* d = gv->dev;
+  char magic[8];
+  int h[8];
+  double phys[8];
+  int rc = 0;
+  if (fread(magic, 1, 8, fp) != 8 || memcmp(magic, LBIB_RESTART_MAGIC, 8) || fread(h, sizeof(h), 1, fp) != 1 ||
+      fread(phys, sizeof(phys), 1, fp) != 1)
+    rc = LBIB_E_IO;
+  if (!rc && (h[0] != 1 || h[1] != d->nx || h[2] != d->ny || h[3] != d->nz || h[4] != d->prec ||
+              h[6] != gv->fiber_shape->num_sheets))
+    rc = LBIB_E_ARG;
+  for (int k = 0; !rc && k < gv->fiber_shape->num_sheets; ++k) {
+    int rc2[2];
+    if (fread(rc2, sizeof(rc2), 1, fp) != 1) rc = LBIB_E_IO;
+    else if (rc2[0] != gv->fiber_shape->sheets[k].num_rows || rc2[1] != gv->fiber_shape->sheets[k].num_cols)
+      rc = LBIB_E_ARG;
+  }
+  if (!rc) {
+    /* the saved physics and compat replace the current ones */
+    gv->tau = phys[0]; gv->u_l = phys[1]; gv->rho_l = phys[2]; gv->Ks_l = phys[3]; gv->Kb_l = phys[4];
+    gv->g_l = phys[5]; gv->cs_l = phys[6]; gv->dt = (int)phys[7];
+    gv->lbib_compat = h[5];
+    lbdev_config c;
+    fill_config(gv, &c);
+    rc = lbdev_set_physics(d, &c);
+  }
+  if (!rc) rc = lbdev_load_state(d, fp);
+  fclose(fp);
+  if (!rc) {
+    gv->time = h[7];
+    rc = lbib_sync_to_host(gv);
+  }
+  return rc ? set_error(rc) : LBIB_OK;
+}
+
 /* ---- the step -------------------------------------------------------- */
 
 static int stage(LV lv, int which) {

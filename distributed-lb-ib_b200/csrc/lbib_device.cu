@@ -7,6 +7,7 @@
  * all stream-ordered on one CUDA stream, with no host synchronisation.
  */
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -506,5 +507,99 @@ extern "C" int lbdev_get_nodes(lbib_device* d, double* out) {
 extern "C" int lbdev_set_nodes(lbib_device* d, const double* in) {
   CK(cudaMemcpyAsync(d->nodes, in, sizeof(double) * 12 * d->S, cudaMemcpyHostToDevice, d->stream));
   CK(cudaStreamSynchronize(d->stream));
+  return 0;
+}
+
+/* ---- restart state: everything the next step reads ------------------------
+ * Written and read in this order, raw device bytes:
+ *   ints   parity, cur, have_forces, have_moments, lp_variant; long steps
+ *   f      [19][N] populations in the storage type
+ *   inlet, outlet tables
+ *   tile_count[cur], tile_slot[cur] [ntiles], tile_list[cur] [count],
+ *   Ftile[cur], Utile[cur] [count] slots
+ *   nodes  [S][12]
+ * The caller checks that the state it loads into has the same grid,
+ * precision and sheets. */
+static int put(FILE* fp, const void* p, size_t n) { return fwrite(p, 1, n, fp) == n ? 0 : -7; }
+static int get(FILE* fp, void* p, size_t n) { return fread(p, 1, n, fp) == n ? 0 : -7; }
+
+static int dev_out(lbib_device* d, FILE* fp, const void* dp, size_t n, void* buf, size_t cap) {
+  for (size_t o = 0; o < n; o += cap) {
+    const size_t k = n - o < cap ? n - o : cap;
+    CK(cudaMemcpy(buf, (const char*)dp + o, k, cudaMemcpyDeviceToHost));
+    if (put(fp, buf, k)) return -7;
+  }
+  (void)d;
+  return 0;
+}
+
+static int dev_in(lbib_device* d, FILE* fp, void* dp, size_t n, void* buf, size_t cap) {
+  for (size_t o = 0; o < n; o += cap) {
+    const size_t k = n - o < cap ? n - o : cap;
+    if (get(fp, buf, k)) return -7;
+    CK(cudaMemcpy((char*)dp + o, buf, k, cudaMemcpyHostToDevice));
+  }
+  (void)d;
+  return 0;
+}
+
+extern "C" int lbdev_save_state(lbib_device* d, FILE* fp) {
+  if (!d->nodes || !d->tile_slot[0]) return -4;
+  CK(cudaStreamSynchronize(d->stream));
+  const int c = d->cur;
+  int count = 0;
+  CK(cudaMemcpy(&count, d->tile_count[c], sizeof(int), cudaMemcpyDeviceToHost));
+  const int hdr[6] = {d->parity, c, d->have_forces, d->have_moments, d->lp_variant, count};
+  int rc = put(fp, hdr, sizeof(hdr));
+  if (!rc) rc = put(fp, &d->steps, sizeof(d->steps));
+  const size_t cap = 64u << 20;
+  void* buf = malloc(cap);
+  if (!buf) return -5;
+  const size_t real = LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 ? 8 : 4;
+  const long P = (long)d->ny * d->nz;
+  if (!rc) rc = dev_out(d, fp, d->f, lbdev_pop_bytes(d->prec) * 19 * d->N, buf, cap);
+  if (!rc) rc = dev_out(d, fp, d->inlet, real * 19 * P, buf, cap);
+  if (!rc) rc = dev_out(d, fp, d->outlet, real * 19 * P, buf, cap);
+  if (!rc) rc = dev_out(d, fp, d->tile_slot[c], sizeof(int) * d->ntiles, buf, cap);
+  if (!rc) rc = dev_out(d, fp, d->tile_list[c], sizeof(int) * count, buf, cap);
+  if (!rc) rc = dev_out(d, fp, d->Ftile[c], sizeof(double) * 192 * count, buf, cap);
+  if (!rc) rc = dev_out(d, fp, d->Utile[c], sizeof(double) * 256 * count, buf, cap);
+  if (!rc) rc = dev_out(d, fp, d->nodes, sizeof(double) * 12 * d->S, buf, cap);
+  free(buf);
+  return rc;
+}
+
+extern "C" int lbdev_load_state(lbib_device* d, FILE* fp) {
+  if (!d->nodes || !d->tile_slot[0]) return -4;
+  CK(cudaStreamSynchronize(d->stream));
+  int hdr[6];
+  long steps = 0;
+  if (get(fp, hdr, sizeof(hdr)) || get(fp, &steps, sizeof(steps))) return -7;
+  const int c = hdr[1], count = hdr[5];
+  if ((c & ~1) || count < 0 || count > d->cap || hdr[0] < 0 || hdr[0] > 1) return -1;
+  const size_t cap = 64u << 20;
+  void* buf = malloc(cap);
+  if (!buf) return -5;
+  const size_t real = LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 ? 8 : 4;
+  const long P = (long)d->ny * d->nz;
+  int rc = dev_in(d, fp, d->f, lbdev_pop_bytes(d->prec) * 19 * d->N, buf, cap);
+  if (!rc) rc = dev_in(d, fp, d->inlet, real * 19 * P, buf, cap);
+  if (!rc) rc = dev_in(d, fp, d->outlet, real * 19 * P, buf, cap);
+  if (!rc) rc = dev_in(d, fp, d->tile_slot[c], sizeof(int) * d->ntiles, buf, cap);
+  if (!rc) rc = dev_in(d, fp, d->tile_list[c], sizeof(int) * count, buf, cap);
+  if (!rc) rc = dev_in(d, fp, d->Ftile[c], sizeof(double) * 192 * count, buf, cap);
+  if (!rc) rc = dev_in(d, fp, d->Utile[c], sizeof(double) * 256 * count, buf, cap);
+  if (!rc) rc = dev_in(d, fp, d->nodes, sizeof(double) * 12 * d->S, buf, cap);
+  free(buf);
+  if (rc) return rc;
+  CK(cudaMemcpy(d->tile_count[c], &count, sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemset(d->tile_slot[c ^ 1], 0xff, sizeof(int) * d->ntiles));
+  d->parity = hdr[0];
+  d->cur = c;
+  d->have_forces = hdr[2];
+  d->have_moments = hdr[3];
+  if (hdr[4] >= -1 && hdr[4] < lbdev_variants(d)) d->lp_variant = hdr[4];
+  d->steps = steps;
+  d->have_df1 = d->have_inout = 1;
   return 0;
 }

@@ -20,6 +20,8 @@
 #ifndef LBIB_INTERNAL_H
 #define LBIB_INTERNAL_H
 
+#include <stdio.h>
+
 #include <cuda_runtime_api.h>
 
 #ifdef __cplusplus
@@ -147,6 +149,9 @@ int  lbdev_set_variant(lbib_device* d, int v);
  * fastest, and restores the initial populations; only before the first
  * step.  ms[i] = mean ms per step of variant i (ms may be NULL). */
 int  lbdev_autotune(lbib_device* d, int steps, double* ms, int max_ms, int* best);
+/* Restart state (raw device bytes of everything the next step reads). */
+int  lbdev_save_state(lbib_device* d, FILE* fp);
+int  lbdev_load_state(lbib_device* d, FILE* fp);
 int  lbdev_profile_begin(lbib_device* d);
 int  lbdev_profile_end(lbib_device* d, double* stage_ms, long* steps);
 

@@ -58,6 +58,7 @@ EXPORTED = [
     "lbib_batch_set_variant", "lbib_batch_autotune",
     "lbib_mlp_create", "lbib_mlp_free", "lbib_mlp_param_count", "lbib_mlp_stream", "lbib_mlp_get_params",
     "lbib_mlp_set_params", "lbib_mlp_forward", "lbib_mlp_gradient", "lbib_mlp_train_step", "lbib_mlp_synchronize",
+    "lbib_save_restart", "lbib_load_restart",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -101,6 +102,8 @@ def load() -> C.CDLL:
     lib.lbib_get_force.argtypes = [C.c_void_p] + [_dp] * 3
     lib.lbib_get_df1.argtypes = [C.c_void_p, _dp]
     lib.lbib_conservation_sums.argtypes = [C.c_void_p, _dp]
+    lib.lbib_save_restart.argtypes = [C.c_void_p, C.c_char_p]
+    lib.lbib_load_restart.argtypes = [C.c_void_p, C.c_char_p]
     lib.lbib_kernel_variants.argtypes = [C.c_void_p]
     lib.lbib_set_kernel_variant.argtypes = [C.c_void_p, C.c_int]
     lib.lbib_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
@@ -288,6 +291,13 @@ class Solver:
         best = self.lib.lbib_autotune(self.gv, steps, _ptr(ms), len(ms))
         _check(min(best, 0), "lbib_autotune")
         return best, ms.tolist()
+
+    def save(self, path: str) -> None:
+        """Restart file of the current state (lbib_save_restart)."""
+        _check(self.lib.lbib_save_restart(self.gv, os.fsencode(path)), "lbib_save_restart")
+
+    def load(self, path: str) -> None:
+        _check(self.lib.lbib_load_restart(self.gv, os.fsencode(path)), "lbib_load_restart")
 
     def conservation(self) -> np.ndarray:
         """[mass, x, y, z momentum] of the populations, FP64 fixed-order sums."""

@@ -96,11 +96,30 @@ def features(problems, tfrac) -> np.ndarray:
     return x
 
 
+MAX_DISP = 60.0   # a node further than this from its start is counted as a stopped run
+
+
+def clean(disp, alive):
+    """A snapshot is valid while its run is going and its displacements are
+    finite and bounded (a diverging run blows up before its sheet leaves the
+    grid).  After the last valid snapshot the displacement target is held at
+    that snapshot's value and the stop output is 0."""
+    ok = alive & np.isfinite(disp).all(axis=(2, 3)) & (np.abs(np.nan_to_num(disp, nan=1e9)).max(axis=(2, 3)) <= MAX_DISP)
+    ok = np.cumprod(ok, axis=1).astype(bool)        # once stopped, stays stopped
+    d = np.where(ok[..., None, None], disp, 0.0).astype(np.float32)
+    last = np.maximum(ok.sum(axis=1) - 1, 0)
+    for i in np.nonzero(~ok.all(axis=1))[0]:
+        hold = d[i, last[i]] if ok[i, last[i]] else np.zeros((64, 3), np.float32)
+        d[i, ~ok[i]] = hold
+    return d, ok
+
+
 def training_set(problems, disp, alive):
     n, snaps = alive.shape
+    d, ok = clean(disp, alive)
     tf = np.repeat(((np.arange(snaps) + 1) / snaps)[None, :], n, axis=0).ravel()
     X = features([problems[i] for i in range(n) for _ in range(snaps)], tf)
-    Y = np.concatenate([disp.reshape(n * snaps, 192) / DISP_SCALE, alive.reshape(n * snaps, 1)], axis=1)
+    Y = np.concatenate([d.reshape(n * snaps, 192) / DISP_SCALE, ok.reshape(n * snaps, 1)], axis=1)
     return X, Y.astype(np.float32)
 
 
@@ -177,6 +196,7 @@ def evaluate(nets, problems, steps: int, truth=None) -> Dict:
     if truth is None:
         truth = simulate(problems, steps, steps, "f64")
     tdisp, talive, _, plain_s = truth
+    tdisp, talive = clean(tdisp, talive)
     true_tip = tip_of(tdisp[:, -1])
     true_alive = talive[:, -1]
     rep = ~s["rerun"]
@@ -198,6 +218,7 @@ def evaluate(nets, problems, steps: int, truth=None) -> Dict:
 def main(argv=None) -> int:
     import argparse
     import json
+    import os
 
     ap = argparse.ArgumentParser(description="learned sweep screen")
     ap.add_argument("--train-n", type=int, default=4096)
@@ -205,17 +226,37 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--iters", type=int, default=4000)
+    ap.add_argument("--data", default=None,
+                    help="directory to keep the simulated runs in (reused when present: only the "
+                         "training and the screen run again)")
     a = ap.parse_args(argv)
     out = {}
     tr = draw(a.train_n, 2)
-    disp, alive, stop, gen_s = simulate(tr, a.steps, a.every, "f16-flow")
-    out["training_runs"] = {"n": a.train_n, "seconds": gen_s, "completed": int(alive[:, -1].sum())}
+    ev = draw(a.eval_n, 3)
+    ftr = os.path.join(a.data, "train.npz") if a.data else None
+    fev = os.path.join(a.data, "truth.npz") if a.data else None
+    if ftr and os.path.exists(ftr):
+        z = np.load(ftr)
+        disp, alive, gen_s = z["disp"].astype(np.float32), z["alive"], float(z["seconds"])
+    else:
+        disp, alive, _, gen_s = simulate(tr, a.steps, a.every, "f16-flow")
+        if ftr:
+            os.makedirs(a.data, exist_ok=True)
+            np.savez(ftr, disp=disp.astype(np.float16), alive=alive, seconds=gen_s)
+    out["training_runs"] = {"n": a.train_n, "seconds": gen_s, "completed": int(clean(disp, alive)[1][:, -1].sum())}
     X, Y = training_set(tr, disp, alive)
     t0 = time.perf_counter()
     nets, curves = train(X, Y, iters=a.iters)
     out["training"] = {"samples": int(X.shape[0]), "seconds": time.perf_counter() - t0, "loss_curves": curves}
-    ev = draw(a.eval_n, 3)
-    out["evaluation"] = evaluate(nets, ev, a.steps)
+    truth = None
+    if fev and os.path.exists(fev):
+        z = np.load(fev)
+        truth = (z["disp"], z["alive"], z["stop"], float(z["seconds"]))
+    else:
+        truth = simulate(ev, a.steps, a.steps, "f64")
+        if fev:
+            np.savez(fev, disp=truth[0], alive=truth[1], stop=truth[2], seconds=truth[3])
+    out["evaluation"] = evaluate(nets, ev, a.steps, truth=truth)
     for n in nets:
         n.close()
     print(json.dumps(out))

@@ -289,6 +289,17 @@ int lbib_sync_to_host(GV gv);
  * fluid_grid planes); gv itself and the objects the caller made stay. */
 void lbib_free(GV gv);
 
+/* Restart files (no counterpart in the reference, which can only restart
+ * from its initial state): lbib_save_restart writes everything the next
+ * step reads -- populations in their storage type, inlet/outlet tables,
+ * the previous step's force and moment tiles, the sheets, the step counters,
+ * physics and gv->time -- so that lbib_load_restart into a GV set up with
+ * the same grid, precision and sheet shapes continues the run bit for bit.
+ * Errors: LBIB_E_IO (file), LBIB_E_ARG (a different grid, precision or
+ * sheets), LBIB_E_STATE (no GPU state or sheets yet). */
+int lbib_save_restart(GV gv, const char* path);
+int lbib_load_restart(GV gv, const char* path);
+
 /* Array access for tests, tools and bindings (x-fastest scalar fields,
  * idx = (z*y_dim + y)*x_dim + x; sheet records of 12 doubles in Fibernode
  * order, row-major).  All return LBIB_OK or an error code. */

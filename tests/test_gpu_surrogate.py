@@ -18,13 +18,15 @@ def test_surrogate_learns_and_screens(gpu):
     disp, alive, stop, _ = surrogate.simulate(tr, steps, every, "f16-flow")
     assert disp.shape == (96, 4, 64, 3) and np.abs(disp[:, -1]).max() > 0
     X, Y = surrogate.training_set(tr, disp, alive)
+    assert np.isfinite(X).all() and np.isfinite(Y).all()
     nets, curves = surrogate.train(X, Y, members=2, iters=600, batch=256)
     for c in curves:
         assert c[-1][1] < 0.2 * c[0][1], c
     ev = surrogate.draw(32, 3)
     truth = surrogate.simulate(ev, steps, steps, "f64")
-    true_tip = surrogate.tip_of(truth[0][:, -1])
-    done = truth[1][:, -1]
+    d, ok = surrogate.clean(truth[0], truth[1])
+    true_tip = surrogate.tip_of(d[:, -1])
+    done = ok[:, -1]
     tip, _ = surrogate.predict(nets, ev)
     err_trained = np.abs(tip.mean(axis=0) - true_tip)[done].mean()
     untrained = [lbib.MLP(surrogate.WIDTHS, max_batch=256, seed=100 + m) for m in range(2)]
