@@ -234,7 +234,8 @@ struct lbib_mlp {
   float* part;
   float* d_loss;
   long steps;
-  cudaStream_t stream;
+  cudaStream_t stream;  /* where the work runs: own_stream or the caller's */
+  cudaStream_t own_stream;
 };
 
 namespace {
@@ -376,7 +377,8 @@ lbib_mlp* lbib_mlp_create(int n_layers, const int* widths, int max_batch, unsign
     nw += (long)n->wp[l + 1] * n->wp[l];
   }
   n->np = np;
-  if (!rc && cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking) != cudaSuccess) rc = -2;
+  if (!rc && cudaStreamCreateWithFlags(&n->own_stream, cudaStreamNonBlocking) != cudaSuccess) rc = -2;
+  n->stream = n->own_stream;
   const size_t fp = sizeof(float) * np;
   if (!rc && cudaMalloc(&n->p, fp) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&n->g, fp) != cudaSuccess) rc = -5;
@@ -432,7 +434,7 @@ void lbib_mlp_free(lbib_mlp* n) {
   for (int l = 0; l <= n->L && n->act; ++l) cudaFree(n->act[l]);
   for (int l = 0; l < n->L && n->z; ++l) cudaFree(n->z[l]);
   cudaFree(n->dA); cudaFree(n->dZ); cudaFree(n->part); cudaFree(n->d_loss);
-  if (n->stream) cudaStreamDestroy(n->stream);
+  if (n->own_stream) cudaStreamDestroy(n->own_stream);
   free(n->w); free(n->wp); free(n->woff); free(n->boff); free(n->wbo); free(n->act); free(n->z);
   free(n);
 }
@@ -440,6 +442,17 @@ void lbib_mlp_free(lbib_mlp* n) {
 long lbib_mlp_param_count(lbib_mlp* n) { return n ? abi_count(n) : 0; }
 
 void* lbib_mlp_stream(lbib_mlp* n) { return n ? (void*)n->stream : NULL; }
+
+/* Run on the caller's stream (NULL is the CUDA default stream, as in every
+ * CUDA call), so the caller's writes of X and T are ordered before the
+ * kernels that read them and its allocator may recycle their memory as
+ * soon as later work on that stream starts. */
+int lbib_mlp_set_stream(lbib_mlp* n, void* stream) {
+  if (!n) return LBIB_E_ARG;
+  if (cudaStreamSynchronize(n->stream) != cudaSuccess) return LBIB_E_CUDA;
+  n->stream = (cudaStream_t)stream;
+  return LBIB_OK;
+}
 
 int lbib_mlp_get_params(lbib_mlp* n, float* out) {
   if (!n || !out) return LBIB_E_ARG;

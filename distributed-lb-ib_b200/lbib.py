@@ -58,7 +58,7 @@ EXPORTED = [
     "lbib_batch_set_variant", "lbib_batch_autotune",
     "lbib_mlp_create", "lbib_mlp_free", "lbib_mlp_param_count", "lbib_mlp_stream", "lbib_mlp_get_params",
     "lbib_mlp_set_params", "lbib_mlp_forward", "lbib_mlp_gradient", "lbib_mlp_train_step", "lbib_mlp_synchronize",
-    "lbib_save_restart", "lbib_load_restart",
+    "lbib_save_restart", "lbib_load_restart", "lbib_mlp_set_stream",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -164,6 +164,7 @@ def load() -> C.CDLL:
     lib.lbib_mlp_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, _fp, _fp]
     lib.lbib_mlp_train_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, _fp]
     lib.lbib_mlp_synchronize.argtypes = [C.c_void_p]
+    lib.lbib_mlp_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
 
@@ -436,7 +437,8 @@ class Batch:
 class MLP:
     """The GPU MLP of the sweep surrogate (lbib_mlp_*).  Arrays passed to
     forward / gradient / train_step are CUDA tensors (float32, contiguous,
-    [batch, width]); torch only provides the device memory."""
+    [batch, width]); torch only provides the device memory, and the MLP runs
+    on the torch stream current at construction."""
 
     def __init__(self, widths, max_batch: int = 1024, seed: int = 0):
         lib = load()
@@ -447,6 +449,11 @@ class MLP:
         if not self.h:
             raise LbibError("lbib_mlp_create failed")
         self.max_batch = max_batch
+        # run on torch's current stream: the batches torch gathers are then
+        # ready before the MLP reads them, and not recycled while it does
+        import torch
+        _check(lib.lbib_mlp_set_stream(self.h, C.c_void_p(torch.cuda.current_stream().cuda_stream)),
+               "lbib_mlp_set_stream")
 
     def close(self) -> None:
         if getattr(self, "h", None):

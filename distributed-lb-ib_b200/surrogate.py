@@ -12,17 +12,21 @@ points from default_rng(3); T = 3000 steps.
 Model: inputs (log10 Ks, log10 Kb, tau, u_x, t/T), affinely scaled to about
 [-1, 1]; 4 hidden layers of 256 with GELU; outputs the x, y, z displacement
 of an 8 x 8 subsample of the sheet's nodes (rows and columns 0, 4, 9, 13,
-18, 22, 27, 31) since t = 0, scaled by 1/20, plus one more output: whether
-the run is still going at t (1) or has stopped because its sheet left the
-grid (0) -- many runs of this parameter range do.  Trained by the library's
-own GPU kernels (lbib_mlp_*: BF16 tensor-core GEMMs, Adam), two members with
-different seeds.
+18, 22, 27, 31) since t = 0, scaled by 1/20; trained on the snapshots of
+runs that are still going, two members with different seeds.  Many runs of
+this parameter range stop (their sheet leaves the grid or blows up), so a
+second, small net (4 parameters -> 2 x 64 -> 1) learns whether a run
+reaches T.  Both are trained by the library's own GPU kernels (lbib_mlp_*:
+BF16 tensor-core GEMMs, Adam).
 
-Screen: both members predict every point at t = T.  A point is re-run by the
-plain FP64 solver when it is among the top 5% by predicted tip displacement
-(the points a sweep is after), when the members disagree on its tip by more
-than `disagree` (relative), or when the stop output is undecided (between
-0.2 and 0.8); every other point is reported from the surrogate.  The judge:
+Screen: the nets predict every point at t = T.  A point is re-run by the
+plain FP64 solver when its stop output is undecided, when it is among the
+top 5% of the points predicted to reach T by tip displacement (the points a
+sweep is after), or when the members disagree on its tip by more than a
+threshold; every other point is reported from the surrogate: "stops", or
+its tip.  The two thresholds are calibrated on the last eighth of the
+training runs, which the nets do not train on: the loosest settings at which
+98% of the points the surrogate would report there are right.  The judge:
 the plain FP64 solver on every point, which the report compares against --
 tip displacement = mean x-displacement of the subsample's last row.
 """
@@ -123,48 +127,61 @@ def training_set(problems, disp, alive):
     return X, Y.astype(np.float32)
 
 
-WIDTHS = [5, 256, 256, 256, 256, 193]
+WIDTHS = [5, 256, 256, 256, 256, 192]      # the displacement surrogate
+STOP_WIDTHS = [4, 64, 64, 1]              # does the run reach T? (parameters only)
 
 
-def train(X, Y, members: int = 2, iters: int = 4000, batch: int = 1024, lr: float = 1e-3):
-    """Train `members` nets on the GPU; returns them and the loss curves."""
+def _fit(net, Xd, Yd, iters, batch, lr, seed):
     import torch
-    Xd = torch.from_numpy(X).cuda()
-    Yd = torch.from_numpy(Y).cuda()
-    n = X.shape[0]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    n = Xd.shape[0]
+    curve = []
+    for it in range(iters):
+        idx = torch.randint(0, n, (batch,), device="cuda", generator=g)
+        want = it % 500 == 0 or it == iters - 1
+        loss = net.train_step(Xd[idx].contiguous(), Yd[idx].contiguous(), lr * (0.1 ** (it / iters)),
+                              want_loss=want)
+        if want:
+            curve.append((it, loss))
+    net.synchronize()
+    return curve
+
+
+def train(X, Y, members: int = 2, iters: int = 6000, batch: int = 1024, lr: float = 1e-3):
+    """Train on the GPU: `members` displacement nets on the snapshots of runs
+    still going, and one stop net on each run's fate at T.  X, Y as made by
+    training_set (Y's last column: the run is still going)."""
+    import torch
+    going = Y[:, 192] > 0.5
+    Xd = torch.from_numpy(X[going]).cuda()
+    Yd = torch.from_numpy(np.ascontiguousarray(Y[going, :192])).cuda()
     nets, curves = [], []
     for m in range(members):
         net = lbib.MLP(WIDTHS, max_batch=batch, seed=100 + m)
-        g = torch.Generator(device="cuda")
-        g.manual_seed(1000 + m)
-        curve = []
-        for it in range(iters):
-            idx = torch.randint(0, n, (batch,), device="cuda", generator=g)
-            xb, yb = Xd[idx].contiguous(), Yd[idx].contiguous()
-            step_lr = lr * (0.1 ** (it / iters))
-            want = it % 500 == 0 or it == iters - 1
-            loss = net.train_step(xb, yb, step_lr, want_loss=want)
-            if want:
-                curve.append((it, loss))
-        net.synchronize()
+        curves.append(_fit(net, Xd, Yd, iters, batch, lr, 1000 + m))
         nets.append(net)
-        curves.append(curve)
-    return nets, curves
+    final = X[:, 4] > 1.0 - 1e-6                   # t = T rows, one per run
+    Xs = torch.from_numpy(np.ascontiguousarray(X[final, :4])).cuda()
+    Ys = torch.from_numpy(np.ascontiguousarray(Y[final, 192:193])).cuda()
+    stop = lbib.MLP(STOP_WIDTHS, max_batch=min(batch, Xs.shape[0]), seed=7)
+    curves.append(_fit(stop, Xs, Ys, iters // 2, min(batch, Xs.shape[0]), lr, 77))
+    return (nets, stop), curves
 
 
-def predict(nets, problems):
+def predict(model, problems):
+    """Per member the tip displacement at T, and the probability-like stop
+    output (1: reaches T)."""
     import torch
+    nets, stop = model
     X = torch.from_numpy(features(problems, np.ones(len(problems)))).cuda()
-    outs = []
-    for net in nets:
-        Y = []
-        for c0 in range(0, X.shape[0], net.max_batch):
-            Y.append(net.forward(X[c0:c0 + net.max_batch].contiguous()))
-        outs.append(torch.cat(Y).cpu().numpy())
-    outs = np.stack(outs)                         # [members, n, 193]
-    disp = outs[..., :192].reshape(len(nets), len(problems), 64, 3) * DISP_SCALE
-    tip = disp[..., 56:64, 0].mean(axis=-1)       # last subsample row, x
-    alive = outs[..., 192]
+    def run(net, X):
+        return torch.cat([net.forward(X[c0:c0 + net.max_batch].contiguous())
+                          for c0 in range(0, X.shape[0], net.max_batch)]).cpu().numpy()
+    outs = np.stack([run(net, X) for net in nets])          # [members, n, 192]
+    disp = outs.reshape(len(nets), len(problems), 64, 3) * DISP_SCALE
+    tip = disp[..., 56:64, 0].mean(axis=-1)                  # last subsample row, x
+    alive = run(stop, X[:, :4].contiguous())[:, 0]
     return tip, alive
 
 
@@ -172,23 +189,58 @@ def tip_of(disp_final: np.ndarray) -> np.ndarray:
     return disp_final[:, 56:64, 0].mean(axis=-1)
 
 
-def screen(nets, problems, top: float = 0.05, disagree: float = 0.02):
-    """Which points the surrogate reports and which go to the plain solver."""
+def calibrate(model, problems, disp_final, going, target: float = 0.98) -> Dict:
+    """Re-run thresholds from runs the nets did not train on: the widest
+    stop band edge and the largest member disagreement at which the points
+    the surrogate would report are still right at `target` rate (stop
+    right; tip within 2%)."""
+    tip, alive = predict(model, problems)
+    m_tip = tip.mean(axis=0)
+    spread = np.abs(tip.max(axis=0) - tip.min(axis=0)) / np.maximum(np.abs(m_tip), 1e-3)
+    true_tip = tip_of(disp_final)
+    tip_ok = np.abs(m_tip - true_tip) <= np.maximum(0.02 * np.abs(true_tip), 0.02)
+    band = 0.3
+    for b in (0.05, 0.1, 0.15, 0.2, 0.25, 0.3, 0.35, 0.4, 0.45):
+        decided = np.abs(alive - 0.5) >= b
+        if decided.any() and ((alive[decided] > 0.5) == going[decided]).mean() >= target:
+            band = b
+            break
+    goes = (alive - 0.5 >= band) & going
+    disagree = 0.0
+    for d in np.sort(spread[goes]):
+        kept = goes & (spread <= d)
+        if tip_ok[kept].mean() >= target:
+            disagree = float(d)
+    return {"stop_band": band, "disagree": disagree}
+
+
+def screen(model, problems, top: float = 0.05, disagree: float = 0.01, band: float = 0.3):
+    """Which points the surrogate reports and which go to the plain solver:
+    stop outputs within `band` of 0.5, the top `top` by predicted tip, and
+    points whose members disagree by more than `disagree` (relative) are
+    re-run."""
     t0 = time.perf_counter()
-    tip, alive = predict(nets, problems)
-    m_tip, m_alive = tip.mean(axis=0), alive.mean(axis=0)
-    spread = np.abs(tip[0] - tip[-1]) / np.maximum(np.abs(m_tip), 1e-3)
-    rerun = spread > disagree
-    rerun |= (m_alive > 0.2) & (m_alive < 0.8)
+    tip, alive = predict(model, problems)
+    m_tip = tip.mean(axis=0)
+    spread = np.abs(tip.max(axis=0) - tip.min(axis=0)) / np.maximum(np.abs(m_tip), 1e-3)
+    goes = alive > 0.5
+    undecided = np.abs(alive - 0.5) < band
+    disagreeing = goes & ~undecided & (spread > disagree)
     k = max(1, int(round(top * len(problems))))
-    rerun[np.argsort(-np.abs(m_tip))[:k]] = True
-    return {"tip": m_tip, "alive": m_alive > 0.5, "rerun": rerun, "seconds": time.perf_counter() - t0}
+    cand = np.where(goes, np.abs(m_tip), -1.0)
+    topk = np.zeros(len(problems), dtype=bool)
+    topk[np.argsort(-cand)[:k]] = True
+    rerun = undecided | disagreeing | topk
+    return {"tip": m_tip, "alive": goes, "spread": spread, "rerun": rerun, "seconds": time.perf_counter() - t0,
+            "why": {"undecided_stop": int(undecided.sum()), "disagreement": int(disagreeing.sum()),
+                    "top": int(topk.sum())}}
 
 
-def evaluate(nets, problems, steps: int, truth=None) -> Dict:
+def evaluate(model, problems, steps: int, truth=None, thresholds=None) -> Dict:
     """Screen `problems`, re-run the flagged ones with the plain FP64 solver,
     and judge every reported point against the plain solver's own run."""
-    s = screen(nets, problems)
+    th = thresholds or {}
+    s = screen(model, problems, disagree=th.get("disagree", 0.01), band=th.get("stop_band", 0.3))
     idx = np.nonzero(s["rerun"])[0]
     rerun_s = 0.0
     if len(idx):
@@ -203,16 +255,19 @@ def evaluate(nets, problems, steps: int, truth=None) -> Dict:
     # a reported point is right when it gets "stopped" right, and, for a run
     # that completes, its tip within 2% (or 0.02 lattice units for tiny tips)
     tip_ok = np.abs(s["tip"] - true_tip) <= np.maximum(0.02 * np.abs(true_tip), 0.02)
+    rel = np.abs(s["tip"] - true_tip) / np.maximum(np.abs(true_tip), 1e-3)
     right = (s["alive"] == true_alive) & (~true_alive | tip_ok)
     sur_s = s["seconds"] + rerun_s
-    return {"points": len(problems), "reported_by_surrogate": int(rep.sum()), "rerun": int(len(idx)),
+    return {"points": len(problems), "reported_by_surrogate": int(rep.sum()), "rerun": int(len(idx)), "rerun_why": s["why"],
             "plain_fp64_s": plain_s, "plain_points_per_s": len(problems) / plain_s,
             "surrogate_s": sur_s, "surrogate_points_per_s": len(problems) / sur_s,
             "speedup": plain_s / sur_s,
             "reported_right": int(right[rep].sum()), "reported_right_frac": float(right[rep].mean()) if rep.any() else 1.0,
             "reported_completed": int((rep & true_alive).sum()),
             "reported_completed_tip_within_2pct": int((rep & true_alive & tip_ok).sum()),
-            "stop_prediction_accuracy": float((s["alive"] == true_alive).mean())}
+            "stop_prediction_accuracy": float((s["alive"] == true_alive).mean()),
+            "all_completed_tip_rel_err_median": float(np.median(rel[true_alive])) if true_alive.any() else None,
+            "all_completed_tip_within_2pct_frac": float((rel[true_alive] <= 0.02).mean()) if true_alive.any() else None}
 
 
 def main(argv=None) -> int:
@@ -225,7 +280,7 @@ def main(argv=None) -> int:
     ap.add_argument("--eval-n", type=int, default=2048)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--every", type=int, default=100)
-    ap.add_argument("--iters", type=int, default=4000)
+    ap.add_argument("--iters", type=int, default=10000)
     ap.add_argument("--data", default=None,
                     help="directory to keep the simulated runs in (reused when present: only the "
                          "training and the screen run again)")
@@ -244,10 +299,16 @@ def main(argv=None) -> int:
             os.makedirs(a.data, exist_ok=True)
             np.savez(ftr, disp=disp.astype(np.float16), alive=alive, seconds=gen_s)
     out["training_runs"] = {"n": a.train_n, "seconds": gen_s, "completed": int(clean(disp, alive)[1][:, -1].sum())}
-    X, Y = training_set(tr, disp, alive)
+    nval = a.train_n // 8                      # the last runs calibrate the screen
+    ntr = a.train_n - nval
+    X, Y = training_set(tr[:ntr], disp[:ntr], alive[:ntr])
     t0 = time.perf_counter()
-    nets, curves = train(X, Y, iters=a.iters)
-    out["training"] = {"samples": int(X.shape[0]), "seconds": time.perf_counter() - t0, "loss_curves": curves}
+    model, curves = train(X, Y, iters=a.iters)
+    out["training"] = {"runs": ntr, "samples": int(X.shape[0]), "seconds": time.perf_counter() - t0,
+                       "loss_curves": curves}
+    dv, okv = clean(disp[ntr:], alive[ntr:])
+    th = calibrate(model, tr[ntr:], dv[:, -1], okv[:, -1])
+    out["calibration"] = dict(th, runs=nval)
     truth = None
     if fev and os.path.exists(fev):
         z = np.load(fev)
@@ -256,8 +317,8 @@ def main(argv=None) -> int:
         truth = simulate(ev, a.steps, a.steps, "f64")
         if fev:
             np.savez(fev, disp=truth[0], alive=truth[1], stop=truth[2], seconds=truth[3])
-    out["evaluation"] = evaluate(nets, ev, a.steps, truth=truth)
-    for n in nets:
+    out["evaluation"] = evaluate(model, ev, a.steps, truth=truth, thresholds=th)
+    for n in model[0] + [model[1]]:
         n.close()
     print(json.dumps(out))
     return 0

@@ -433,12 +433,17 @@ int lbib_batch_autotune(lbib_batch* b, int steps, double* ms, int max_ms, int* c
  * 0.9, beta2 0.999, eps 1e-8).  Parameters, in order: per layer W
  * [out][in] row-major, then b [out].  X, T, Y of forward/train/gradient are
  * device pointers to row-major FP32 [batch][width] arrays; grad and loss of
- * lbib_mlp_gradient are host memory.  Returns NULL / error codes as above. */
+ * lbib_mlp_gradient are host memory; the work runs on the MLP's stream.
+ * Returns NULL / error codes as above. */
 typedef struct lbib_mlp lbib_mlp;
 lbib_mlp* lbib_mlp_create(int n_layers, const int* widths, int max_batch, unsigned long long seed);
 void lbib_mlp_free(lbib_mlp* n);
 long lbib_mlp_param_count(lbib_mlp* n);
 void* lbib_mlp_stream(lbib_mlp* n);
+/* Run on the caller's CUDA stream (NULL: the CUDA default stream); the MLP
+ * starts on a stream of its own.  Inputs written by the caller on another
+ * stream must be ready before the MLP reads them. */
+int lbib_mlp_set_stream(lbib_mlp* n, void* stream);
 int lbib_mlp_get_params(lbib_mlp* n, float* out);
 int lbib_mlp_set_params(lbib_mlp* n, const float* in);
 int lbib_mlp_forward(lbib_mlp* n, const float* X, int batch, float* Y);

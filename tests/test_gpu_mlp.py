@@ -61,3 +61,23 @@ def test_adam_training_fits_a_smooth_map(gpu):
             net.train_step(Xd[k:k + 512], Td[k:k + 512], 3e-3)
         last = net.train_step(Xd[:512], Td[:512], 3e-3, want_loss=True)
     assert last < 0.05 * first, (first, last)
+
+
+def test_training_on_fresh_gathered_batches(gpu):
+    """Batches gathered by torch just before each step (temporaries on
+    torch's stream) must be what the MLP trains on."""
+    import torch
+    rng = np.random.default_rng(5)
+    X = rng.uniform(-1, 1, (8192, 5)).astype(np.float32)
+    T = np.tanh(X @ rng.normal(0, 1, (5, 24))).astype(np.float32)
+    Xd, Td = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    with lbib.MLP([5, 64, 64, 24], max_batch=1024, seed=7) as net:
+        first = None
+        for it in range(800):
+            idx = torch.randint(0, 8192, (1024,), device="cuda", generator=g)
+            loss = net.train_step(Xd[idx].contiguous(), Td[idx].contiguous(), 3e-3, want_loss=it in (0, 799))
+            if it == 0:
+                first = loss
+        assert loss < 0.02 * first, (first, loss)
