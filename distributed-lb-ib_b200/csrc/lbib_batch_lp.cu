@@ -38,25 +38,9 @@ int words(const BatchFluid& f, const int2* blk, long nblk) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-/* The one-grid autotuner's table: 16-bit {V, MINB} = {4,3} {4,4} {2,4}
- * {2,5} {2,6}; FP32 {2,3} {2,4} {2,5}. */
 template <typename T>
 int words_v(const BatchFluid& f, int v, const int2* blk, long nblk) {
-  if constexpr (sizeof(T) == 2) {
-    switch (v) {
-      case 1: return words<T, 4, 4>(f, blk, nblk);
-      case 2: return words<T, 2, 4>(f, blk, nblk);
-      case 3: return words<T, 2, 5>(f, blk, nblk);
-      case 4: return words<T, 2, 6>(f, blk, nblk);
-      default: return words<T, 4, 3>(f, blk, nblk);
-    }
-  } else {
-    switch (v) {
-      case 1: return words<T, 2, 4>(f, blk, nblk);
-      case 2: return words<T, 2, 5>(f, blk, nblk);
-      default: return words<T, 2, 3>(f, blk, nblk);
-    }
-  }
+  return with_variant<T>(v, [&](auto V, auto MINB) { return words<T, V, MINB>(f, blk, nblk); });
 }
 
 template <typename T>
@@ -89,12 +73,9 @@ int batch_words_lp(const BatchFluid& f, int variant, const int2* blk, long nblk)
   }
 }
 
-int batch_variants_lp(int prec) { return LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? 3 : 5; }
+int batch_variants_lp(int prec) { return word_variants(prec); }
 
-int batch_variant_cells_lp(int prec, int variant) {
-  if (LBIB_PREC_TYPE(prec) == LBIB_PREC_F32) return 2;
-  return (variant == 0 || variant == 1) ? 4 : 2;
-}
+int batch_variant_cells_lp(int prec, int variant) { return word_variant_cells(prec, variant); }
 
 int batch_tile_moments_lp(const BatchFluid& f) {
   switch (LBIB_PREC_TYPE(f.prec)) {

@@ -82,34 +82,13 @@ int launch_words(lbib_device* d, const FluidParamsT<T>& p) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-/* Word-kernel variants the autotuner chooses from: cells per thread and
- * the resident blocks per SM the registers are sized for.  (A variant that
- * prefetched the next rows' words into shared memory with cp.async measured
- * no faster and was dropped.) */
-constexpr int kN16 = 5;  /* {V, MINB}: {4,3} {4,4} {2,4} {2,5} {2,6} */
-constexpr int kN32 = 3;  /* {2,3} {2,4} {2,5} */
-
 template <typename T>
 int lp_step(lbib_device* d) {
   FluidParamsT<T> p = make_params_t<T>(d, d->steps == 0);
   if (launch_step_rows_t<T>(d, p)) return -2;
   if (!d->use_bulk) return 0;
-  const int i = d->lp_variant < 0 ? 0 : d->lp_variant;
-  if constexpr (sizeof(T) == 2) {
-    switch (i) {
-      case 1: return launch_words<T, 4, 4>(d, p);
-      case 2: return launch_words<T, 2, 4>(d, p);
-      case 3: return launch_words<T, 2, 5>(d, p);
-      case 4: return launch_words<T, 2, 6>(d, p);
-      default: return launch_words<T, 4, 3>(d, p);
-    }
-  } else {
-    switch (i) {
-      case 1: return launch_words<T, 2, 4>(d, p);
-      case 2: return launch_words<T, 2, 5>(d, p);
-      default: return launch_words<T, 2, 3>(d, p);
-    }
-  }
+  return with_variant<T>(d->lp_variant < 0 ? 0 : d->lp_variant,
+                         [&](auto V, auto MINB) { return launch_words<T, V, MINB>(d, p); });
 }
 
 }  // namespace
@@ -170,10 +149,5 @@ extern "C" int lbdev_lp_sums(lbib_device* d, double* part, double* out) {
 
 /* Word-kernel variants available for a precision (1 for FP64). */
 extern "C" int lbdev_lp_variants(int prec) {
-  switch (LBIB_PREC_TYPE(prec)) {
-    case LBIB_PREC_F32: return kN32;
-    case LBIB_PREC_F16:
-    case LBIB_PREC_BF16: return kN16;
-    default: return 1;
-  }
+  return LBIB_PREC_TYPE(prec) == LBIB_PREC_F64 ? 1 : word_variants(prec);
 }

@@ -179,6 +179,86 @@ __device__ __forceinline__ const void* edge_src(const typename Word<T, V>::U* sr
   return (const void*)(src + V);
 }
 
+/* Two FP32 lanes in one 64-bit register, for sm_100's packed FP32
+ * add / sub / mul / fma (each lane rounds as the scalar instruction does):
+ * the word kernel collides two neighbouring cells with one instruction. */
+struct F2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float a, float b) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ F2 f2(float a) { return f2(a, a); }
+__device__ __forceinline__ void split(F2 x, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v)); }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+/* a * b + c */
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+/* Form<T, true>::moments_free and collide<false> for two cells at once,
+ * the same operations lane by lane. */
+template <typename P>
+__device__ __forceinline__ void moments_free2(const F2 d[19], const P& p, F2& drho, F2& dux, F2& duy, F2& duz) {
+  const F2 m0 = ((d[0] + d[1]) + (d[2] + d[3])) + ((d[4] + d[5]) + (d[6] + d[7]));
+  const F2 m1 = ((d[8] + d[9]) + (d[10] + d[11])) + ((d[12] + d[13]) + (d[14] + d[15]));
+  drho = (m0 + m1) + ((d[16] + d[17]) + d[18]);
+  const F2 jx = ((d[1] - d[2]) + (d[7] - d[8])) + ((d[9] - d[10]) + (d[15] - d[16])) + (d[17] - d[18]);
+  const F2 jy = ((d[6] - d[5]) + (d[12] - d[11])) + ((d[13] - d[14]) + (d[16] - d[15])) + (d[17] - d[18]);
+  const F2 jz = ((d[3] - d[4]) + (d[7] - d[8])) + ((d[10] - d[9]) + (d[11] - d[12])) + (d[13] - d[14]);
+  float r0, r1;
+  split(f2(p.frs) + drho, r0, r1);
+  const F2 inv = f2(__frcp_rn(r0), __frcp_rn(r1));
+  dux = fma2(drho, f2(-p.fus), jx) * inv;
+  duy = jy * inv;
+  duz = jz * inv;
+}
+
+template <int QA, int QB, typename P>
+__device__ __forceinline__ void lp_pair2(F2* d, F2 a, F2 itw, F2 drho, F2 rho, F2 t, F2 om, const P& p) {
+  const F2 sq = fma2(f2(4.5f) * a, a, f2(0.0f) - t);
+  const F2 xa = fma2(rho, fma2(f2(3.0f), a, sq), drho - f2(p.fC[QA]));
+  const F2 xb = fma2(rho, fma2(f2(-3.0f), a, sq), drho - f2(p.fC[QB]));
+  d[QA] = fma2(d[QA], om, itw * xa);
+  d[QB] = fma2(d[QB], om, itw * xb);
+}
+
+template <typename P>
+__device__ __forceinline__ void collide2(F2 d[19], F2 drho, F2 dux, F2 duy, F2 duz, const P& p) {
+  const F2 rho = f2(p.frs) + drho;
+  const F2 ux = f2(p.fus) + dux, uy = duy, uz = duz;
+  const F2 t = f2(1.5f) * fma2(ux, ux, fma2(uy, uy, uz * uz));
+  const F2 om = f2(p.fom), i1 = f2(p.fitw1), i2 = f2(p.fitw2);
+  d[0] = fma2(d[0], om, f2(p.fitw0) * ((drho - f2(p.fC[0])) - rho * t));
+  lp_pair2<1, 2>(d, ux, i1, drho, rho, t, om, p);
+  lp_pair2<3, 4>(d, uz, i1, drho, rho, t, om, p);
+  lp_pair2<6, 5>(d, uy, i1, drho, rho, t, om, p);
+  lp_pair2<7, 8>(d, ux + uz, i2, drho, rho, t, om, p);
+  lp_pair2<9, 10>(d, ux - uz, i2, drho, rho, t, om, p);
+  lp_pair2<11, 12>(d, uz - uy, i2, drho, rho, t, om, p);
+  lp_pair2<13, 14>(d, uy + uz, i2, drho, rho, t, om, p);
+  lp_pair2<15, 16>(d, ux - uy, i2, drho, rho, t, om, p);
+  lp_pair2<17, 18>(d, ux + uy, i2, drho, rho, t, om, p);
+}
+
 /* Collide the V cells and store them (AA pushes assembled across lanes). */
 template <typename T, int V, int PAR>
 __device__ __forceinline__ void words_collide_store(const FluidParamsT<T>& p, const ItemCtx& c, int lane, float* d) {
@@ -191,17 +271,27 @@ __device__ __forceinline__ void words_collide_store(const FluidParamsT<T>& p, co
     const int c0 = cell_in_tile(c.x0, c.y, c.z);
     const int sp = p.first ? -1 : p.slot_prev[tile];
 #pragma unroll
-    for (int e = 0; e < V; ++e) {
-      float f[19];
+    for (int e = 0; e < V; e += 2) {
+      F2 f[19];
 #pragma unroll
-      for (int q = 0; q < 19; ++q) f[q] = d[q * V + e];
-      Mom<float> m;
-      if (p.first) Fm::initial(p, m);
-      else if (sp >= 0) Fm::from_tile(p, p.Uprev + (long)sp * 256, c0 + e, m);
-      else Fm::moments_free(f, p, m);
-      Fm::template collide<false>(f, m, 0.0f, 0.0f, 0.0f, p);
+      for (int q = 0; q < 19; ++q) f[q] = f2(d[q * V + e], d[q * V + e + 1]);
+      F2 drho, dux, duy, duz;
+      if (p.first || sp >= 0) {
+        Mom<float> m0, m1;
+        if (p.first) {
+          Fm::initial(p, m0);
+          m1 = m0;
+        } else {
+          Fm::from_tile(p, p.Uprev + (long)sp * 256, c0 + e, m0);
+          Fm::from_tile(p, p.Uprev + (long)sp * 256, c0 + e + 1, m1);
+        }
+        drho = f2(m0.rho, m1.rho); dux = f2(m0.ux, m1.ux); duy = f2(m0.uy, m1.uy); duz = f2(m0.uz, m1.uz);
+      } else {
+        moments_free2(f, p, drho, dux, duy, duz);
+      }
+      collide2(f, drho, dux, duy, duz, p);
 #pragma unroll
-      for (int q = 0; q < 19; ++q) d[q * V + e] = f[q];
+      for (int q = 0; q < 19; ++q) split(f[q], d[q * V + e], d[q * V + e + 1]);
     }
   }
   U* __restrict__ F = reinterpret_cast<U*>(p.f);
@@ -300,6 +390,42 @@ __device__ __forceinline__ void edge_cell(const FluidParamsT<T>& p, int nry, int
   const int y = 3 + r % nry, z = 3 + r / nry;
   const int x = k < 2 ? 2 + k : p.nx - 6 + k;
   step_cell<T, PAR>(p, x, y, z);
+}
+
+/* The word-kernel variants that the one-grid and the batched launches and
+ * their autotuners choose from: {cells per thread V, resident blocks per SM
+ * the registers are sized for}.  16-bit storage: {4,3} {4,4} {2,4} {2,5}
+ * {2,6}; FP32: {2,3} {2,4} {2,5}.  (A variant that prefetched the next rows'
+ * words into shared memory with cp.async measured no faster and was
+ * dropped.)  with_variant calls f(V, MINB) as integral constants. */
+constexpr int kWordVariants16 = 5, kWordVariants32 = 3;
+
+__host__ __forceinline__ int word_variants(int prec) {
+  return LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? kWordVariants32 : kWordVariants16;
+}
+
+__host__ __forceinline__ int word_variant_cells(int prec, int v) {
+  return LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? 2 : (v <= 1 ? 4 : 2);
+}
+
+template <typename T, typename F>
+int with_variant(int v, F&& f) {
+  using std::integral_constant;
+  if constexpr (sizeof(T) == 2) {
+    switch (v) {
+      case 1: return f(integral_constant<int, 4>{}, integral_constant<int, 4>{});
+      case 2: return f(integral_constant<int, 2>{}, integral_constant<int, 4>{});
+      case 3: return f(integral_constant<int, 2>{}, integral_constant<int, 5>{});
+      case 4: return f(integral_constant<int, 2>{}, integral_constant<int, 6>{});
+      default: return f(integral_constant<int, 4>{}, integral_constant<int, 3>{});
+    }
+  } else {
+    switch (v) {
+      case 1: return f(integral_constant<int, 2>{}, integral_constant<int, 4>{});
+      case 2: return f(integral_constant<int, 2>{}, integral_constant<int, 5>{});
+      default: return f(integral_constant<int, 2>{}, integral_constant<int, 3>{});
+    }
+  }
 }
 
 /* Bulk-row geometry of a grid for the word kernel with V cells per word. */
