@@ -194,8 +194,8 @@ struct lbib_batch {
   int4* rows;
   long nrows;
   int max_nx;
-  long* edge_off;
-  long nedge;
+  int2* eblk;                    /* edge-cell blocks (problem, first bulk row) */
+  long neblk;
   int* variant;                  /* word-kernel variant per problem */
   int2* wblk[MAXV];              /* word blocks of each variant group */
   long nwblk[MAXV];
@@ -301,10 +301,9 @@ int build_rows(lbib_batch* b) {
   long n = 0;
   for (int k = 0; k < b->B; ++k) n += (long)(b->sh[k]->ny - 4) * (b->sh[k]->nz - 4);
   int4* h = (int4*)malloc(sizeof(int4) * (n ? n : 1));
-  long* eo = (long*)malloc(sizeof(long) * (b->B + 1));
+  int2* eo = (int2*)malloc(sizeof(int2) * (n / 32 + b->B + 1));
   if (!h || !eo) { free(h); free(eo); return -5; }
-  long r = 0;
-  eo[0] = 0;
+  long r = 0, ne = 0;
   b->max_nx = 0;
   for (int k = 0; k < b->B; ++k) {
     lbib_device* d = b->sh[k];
@@ -316,16 +315,17 @@ int build_rows(lbib_batch* b) {
         const int in_bulk = bulk && y >= 3 && y <= d->ny - 4 && z >= 3 && z <= zb;
         if (!in_bulk) h[r++] = make_int4(k, y, z, 0);
       }
-    eo[k + 1] = eo[k] + (bulk ? 4L * ry * rz : 0);
+    if (bulk)
+      for (long r0 = 0; r0 < (long)ry * rz; r0 += 32) eo[ne++] = make_int2(k, (int)r0);
     if (d->nx > b->max_nx) b->max_nx = d->nx;
   }
   b->nrows = r;
-  b->nedge = eo[b->B];
+  b->neblk = ne;
   int rc = 0;
   if (cudaMalloc(&b->rows, sizeof(int4) * (r ? r : 1)) != cudaSuccess) rc = -5;
   else if (r && cudaMemcpy(b->rows, h, sizeof(int4) * r, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
-  if (!rc && cudaMalloc(&b->edge_off, sizeof(long) * (b->B + 1)) != cudaSuccess) rc = -5;
-  else if (!rc && cudaMemcpy(b->edge_off, eo, sizeof(long) * (b->B + 1), cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
+  if (!rc && cudaMalloc(&b->eblk, sizeof(int2) * (ne ? ne : 1)) != cudaSuccess) rc = -5;
+  else if (!rc && ne && cudaMemcpy(b->eblk, eo, sizeof(int2) * ne, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
   free(h);
   free(eo);
   return rc;
@@ -343,8 +343,8 @@ BatchFluid fluid_args(lbib_batch* b, int par, const void* P, const void* WP, int
   f.rows = b->rows;
   f.nrows = b->nrows;
   f.max_nx = b->max_nx;
-  f.edge_off = b->edge_off;
-  f.nedge = b->nedge;
+  f.eblk = b->eblk;
+  f.neblk = b->neblk;
   f.list = b->tile_list[c];
   f.count = b->tile_count[c];
   f.tile_inst = b->tile_inst;
@@ -676,7 +676,7 @@ void lbib_batch_free(lbib_batch* b) {
   cudaFree(b->err);
   cudaFree(b->step_no);
   if (b->h_err) cudaFreeHost(b->h_err);
-  cudaFree(b->desc); cudaFree(b->rows); cudaFree(b->edge_off);
+  cudaFree(b->desc); cudaFree(b->rows); cudaFree(b->eblk);
   for (int v = 0; v < MAXV; ++v) cudaFree(b->wblk[v]);
   if (b->stream) cudaStreamDestroy(b->stream);
   free(b->prob); free(b->h_desc); free(b->variant);

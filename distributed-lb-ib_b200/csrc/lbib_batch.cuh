@@ -9,8 +9,8 @@
  * compaction serve the whole batch.  Work is enumerated across problems:
  *   rows     (problem, y, z) of the rows the generic kernel takes;
  *   words    blocks of the word kernel, (problem, block within problem);
- *   edges    the cells x in {2, 3, nx-4, nx-3} of bulk rows, as a prefix
- *            over problems;
+ *   edges    the cells x in {2, 3, nx-4, nx-3} of bulk rows, blocks of
+ *            (problem, 32 rows);
  *   tiles    the global touched-tile list, tile -> problem by a table.
  * A problem whose error word is set (a fiber stencil left its grid) is
  * skipped by every kernel from then on; the others continue.
@@ -71,28 +71,18 @@ __global__ void __launch_bounds__(WTPB, MINB) lbib_b_words(const WordsParams<T>*
   words_item<T, V, PAR>(sb, (long)m.y * WTPB + threadIdx.x);
 }
 
-/* Largest i with off[i] <= t (off ascending, off[0] = 0, n entries). */
-__device__ __forceinline__ int find_slice(const long* __restrict__ off, int n, long t) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (off[mid] <= t) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
-/* Edge cells: thread t -> problem by the prefix edge_off[0..B] of 4 * bulk
- * rows per problem. */
+/* Edge cells: a block per (problem, 32 bulk rows), 4 cells per row. */
 template <typename T, int PAR>
 __global__ void __launch_bounds__(128) lbib_b_edges(const FluidParamsT<T>* __restrict__ P,
                                                     const WordsParams<T>* __restrict__ WP,
-                                                    const long* __restrict__ edge_off, int B, const int* __restrict__ err) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= edge_off[B]) return;
-  const int k = find_slice(edge_off, B + 1, t);
-  if (err[2 * k] || edge_off[k + 1] == edge_off[k]) return;
-  const long e = t - edge_off[k];
-  edge_cell<T, PAR>(P[k], WP[k].nry, (int)(e >> 2), (int)(e & 3));
+                                                    const int2* __restrict__ blk, const int* __restrict__ err) {
+  __shared__ __align__(16) FluidParamsT<T> sp;
+  const int2 m = blk[blockIdx.x];
+  if (err[2 * m.x]) return;
+  block_copy(sp, P + m.x);
+  const int r = m.y + (int)(threadIdx.x >> 2);
+  if (r >= WP[m.x].nrows) return;
+  edge_cell<T, PAR>(sp, WP[m.x].nry, r, threadIdx.x & 3);
 }
 
 /* Cells of forced tiles in the word kernel's range, over the global list. */

@@ -24,8 +24,8 @@ struct BatchFluid {
   const int4* rows;        /* generic rows */
   long nrows;
   int max_nx;
-  const long* edge_off;    /* [B + 1] */
-  long nedge;
+  const int2* eblk;        /* edge-cell blocks: (problem, first bulk row) */
+  long neblk;
   const int* list;         /* touched tiles (global ids) */
   const int* count;
   const int* tile_inst;

@@ -19,10 +19,9 @@ int rest(const BatchFluid& f) {
     if (f.par == 0) lbib_b_rows<T, 0><<<grid, 128, 0, f.stream>>>(P, f.rows, f.err);
     else lbib_b_rows<T, 1><<<grid, 128, 0, f.stream>>>(P, f.rows, f.err);
   }
-  if (f.nedge > 0) {
-    const unsigned eb = (unsigned)((f.nedge + 127) / 128);
-    if (f.par == 0) lbib_b_edges<T, 0><<<eb, 128, 0, f.stream>>>(P, WP, f.edge_off, f.B, f.err);
-    else lbib_b_edges<T, 1><<<eb, 128, 0, f.stream>>>(P, WP, f.edge_off, f.B, f.err);
+  if (f.neblk > 0) {
+    if (f.par == 0) lbib_b_edges<T, 0><<<(unsigned)f.neblk, 128, 0, f.stream>>>(P, WP, f.eblk, f.err);
+    else lbib_b_edges<T, 1><<<(unsigned)f.neblk, 128, 0, f.stream>>>(P, WP, f.eblk, f.err);
   }
   if (f.par == 0) lbib_b_forced<T, 0><<<f.grid_tiles, 64, 0, f.stream>>>(P, f.desc, f.list, f.count, f.tile_inst, f.err);
   else lbib_b_forced<T, 1><<<f.grid_tiles, 64, 0, f.stream>>>(P, f.desc, f.list, f.count, f.tile_inst, f.err);

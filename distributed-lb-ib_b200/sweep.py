@@ -105,8 +105,9 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--precision", default="f16-flow")
     ap.add_argument("--free", action="store_true", help="sheets not pinned (the reference's free sheets)")
+    ap.add_argument("--no-autotune", action="store_true", help="default kernel variant for every size class")
     a = ap.parse_args(argv)
-    rep = run_sweep(draw_problems(a.n, a.seed, not a.free), a.steps, a.precision)
+    rep = run_sweep(draw_problems(a.n, a.seed, not a.free), a.steps, a.precision, autotune=not a.no_autotune)
     print(json.dumps(rep))
     return 0
 
