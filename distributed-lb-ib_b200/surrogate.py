@@ -13,7 +13,8 @@ Model: inputs (log10 Ks, log10 Kb, tau, u_x, t/T), affinely scaled to about
 [-1, 1]; 4 hidden layers of 256 with GELU; outputs the x, y, z displacement
 of an 8 x 8 subsample of the sheet's nodes (rows and columns 0, 4, 9, 13,
 18, 22, 27, 31) since t = 0, scaled by 1/20; trained on the snapshots of
-runs that are still going, two members with different seeds.  Many runs of
+runs that are still going, three members, each on its own bootstrap of the
+training runs.  Many runs of
 this parameter range stop (their sheet leaves the grid or blows up), so a
 second, small net (4 parameters -> 2 x 64 -> 1) learns whether a run
 reaches T.  Both are trained by the library's own GPU kernels (lbib_mlp_*:
@@ -148,20 +149,27 @@ def _fit(net, Xd, Yd, iters, batch, lr, seed):
     return curve
 
 
-def train(X, Y, members: int = 2, iters: int = 6000, batch: int = 1024, lr: float = 1e-3):
+def train(X, Y, members: int = 3, iters: int = 6000, batch: int = 1024, lr: float = 1e-3):
     """Train on the GPU: `members` displacement nets on the snapshots of runs
     still going, and one stop net on each run's fate at T.  X, Y as made by
     training_set (Y's last column: the run is still going)."""
     import torch
+    final = X[:, 4] > 1.0 - 1e-6                   # t = T rows, one per run
+    runs = int(final.sum())
+    run_of_row = np.arange(X.shape[0]) // (X.shape[0] // runs)
     going = Y[:, 192] > 0.5
-    Xd = torch.from_numpy(X[going]).cuda()
-    Yd = torch.from_numpy(np.ascontiguousarray(Y[going, :192])).cuda()
     nets, curves = [], []
     for m in range(members):
+        # each member sees its own bootstrap of the runs, so that their
+        # disagreement tracks how well the data pins a point down
+        pick = np.zeros(runs, dtype=bool)
+        pick[np.random.default_rng(500 + m).integers(0, runs, runs)] = True
+        rows = going & pick[run_of_row]
+        Xd = torch.from_numpy(np.ascontiguousarray(X[rows])).cuda()
+        Yd = torch.from_numpy(np.ascontiguousarray(Y[rows, :192])).cuda()
         net = lbib.MLP(WIDTHS, max_batch=batch, seed=100 + m)
         curves.append(_fit(net, Xd, Yd, iters, batch, lr, 1000 + m))
         nets.append(net)
-    final = X[:, 4] > 1.0 - 1e-6                   # t = T rows, one per run
     Xs = torch.from_numpy(np.ascontiguousarray(X[final, :4])).cuda()
     Ys = torch.from_numpy(np.ascontiguousarray(Y[final, 192:193])).cuda()
     stop = lbib.MLP(STOP_WIDTHS, max_batch=min(batch, Xs.shape[0]), seed=7)
