@@ -26,6 +26,7 @@
 #include "lbib_batch.cuh"
 #include "lbib_batch_internal.h"
 #include "lbib_ib.cuh"
+#include "lbib_x2.cuh"
 
 extern "C" {
 int lbdev_bulk_rows(const lbib_device* d, int* nrows_y, int* nrows_z);
@@ -135,13 +136,28 @@ __global__ void lbib_b_move(double* __restrict__ nodes, const double* __restrict
   move_node(nodes, W, st, i, d.ntx, d.nty, slot + d.tile0, Utile, d.dt);
 }
 
+/* FP64 rows away from the walls: the two-cell step, a block per 128 pairs of
+ * a problem's (row, pair) range, the parameters in shared memory. */
+template <int PAR>
+__global__ void __launch_bounds__(128, 3) lbib_b_x2(const FluidParams* __restrict__ P, const int2* __restrict__ blk,
+                                                    const int* __restrict__ err) {
+  __shared__ __align__(16) FluidParams sp;
+  const int2 m = blk[blockIdx.x];
+  if (err[2 * m.x]) return;
+  block_copy(sp, P + m.x);
+  const int npairs = (sp.nx - 4) / 2, nry = sp.ny - 6;
+  const long g = (long)m.y * 128 + threadIdx.x;
+  const long row = g / npairs;
+  if (row >= (long)nry * x2_rows_z(sp.nz, sp.zin_hi)) return;
+  const int pr = (int)(g - row * npairs);
+  x2_pair<PAR>(sp, 2 + 2 * pr, 3 + (int)(row % nry), 3 + (int)(row / nry));
+}
+
 template <int PAR>
 int rest_f64_t(const BatchFluid& f) {
-  const FluidParamsT<double>* P = static_cast<const FluidParamsT<double>*>(f.P);
-  if (f.nrows > 0) {
-    dim3 grid((unsigned)f.nrows, (unsigned)((f.max_nx - 4 + 127) / 128));
-    lbib_b_rows<double, PAR><<<grid, 128, 0, f.stream>>>(P, f.rows, f.err);
-  }
+  const FluidParams* P = static_cast<const FluidParams*>(f.P);
+  if (f.nxblk > 0) lbib_b_x2<PAR><<<(unsigned)f.nxblk, 128, 0, f.stream>>>(P, f.xblk, f.err);
+  if (f.nrblk > 0) lbib_b_rows<double, PAR><<<(unsigned)f.nrblk, 128, 0, f.stream>>>(P, f.rowyz, f.rblk, f.err);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -191,9 +207,11 @@ struct lbib_batch {
   /* per-problem fluid parameters: [cur] with first = 0, and the first step */
   void *P[2], *P_first, *WP[2], *WP_first;
   size_t psize, wsize;
-  int4* rows;
-  long nrows;
-  int max_nx;
+  int2* rowyz;                   /* generic rows (y, z), each problem's contiguous */
+  int4* rblk;                    /* generic-row blocks */
+  long nrblk;
+  int2* xblk;                    /* FP64 two-cell blocks (problem, block) */
+  long nxblk;
   int2* eblk;                    /* edge-cell blocks (problem, first bulk row) */
   long neblk;
   int* variant;                  /* word-kernel variant per problem */
@@ -295,39 +313,63 @@ int build_word_blocks(lbib_batch* b) {
   return 0;
 }
 
-/* Rows of the generic kernel (every row of I for FP64 and for problems
- * without bulk rows; the wall rows otherwise) and the edge-cell prefix. */
+/* Rows of the generic kernel (every row of I for problems without bulk
+ * rows; the wall rows otherwise) and their 128-cell blocks; the bulk rows'
+ * blocks: FP64 two-cell blocks, or the edge-cell blocks of the
+ * low-precision word kernel (whose own blocks build_word_blocks makes). */
 int build_rows(lbib_batch* b) {
-  long n = 0;
-  for (int k = 0; k < b->B; ++k) n += (long)(b->sh[k]->ny - 4) * (b->sh[k]->nz - 4);
-  int4* h = (int4*)malloc(sizeof(int4) * (n ? n : 1));
-  int2* eo = (int2*)malloc(sizeof(int2) * (n / 32 + b->B + 1));
-  if (!h || !eo) { free(h); free(eo); return -5; }
-  long r = 0, ne = 0;
-  b->max_nx = 0;
+  const int lp = is_lp(b);
+  long n = 0, nr = 0, ne = 0, nxb = 0;
   for (int k = 0; k < b->B; ++k) {
-    lbib_device* d = b->sh[k];
+    const lbib_device* d = b->sh[k];
+    int ry = 0, rz = 0;
+    const int bulk = b->h_desc[k].bulk && lbdev_bulk_rows(d, &ry, &rz);
+    const long rows = (long)(d->ny - 4) * (d->nz - 4) - (bulk ? (long)ry * rz : 0);
+    n += rows;
+    nr += (rows * (d->nx - 4) + 127) / 128;
+    if (bulk && lp) ne += ((long)ry * rz + 31) / 32;
+    if (bulk && !lp) nxb += ((long)ry * rz * ((d->nx - 4) / 2) + 127) / 128;
+  }
+  int2* h = (int2*)malloc(sizeof(int2) * (n ? n : 1));
+  int4* rb = (int4*)malloc(sizeof(int4) * (nr ? nr : 1));
+  int2* eo = (int2*)malloc(sizeof(int2) * (ne ? ne : 1));
+  int2* xo = (int2*)malloc(sizeof(int2) * (nxb ? nxb : 1));
+  if (!h || !rb || !eo || !xo) { free(h); free(rb); free(eo); free(xo); return -5; }
+  long r = 0, ir = 0, ie = 0, ix = 0;
+  for (int k = 0; k < b->B; ++k) {
+    const lbib_device* d = b->sh[k];
     int ry = 0, rz = 0;
     const int bulk = b->h_desc[k].bulk && lbdev_bulk_rows(d, &ry, &rz);
     const int zb = 2 + rz;
+    const long r0 = r;
     for (int z = 2; z <= d->nz - 3; ++z)
       for (int y = 2; y <= d->ny - 3; ++y) {
         const int in_bulk = bulk && y >= 3 && y <= d->ny - 4 && z >= 3 && z <= zb;
-        if (!in_bulk) h[r++] = make_int4(k, y, z, 0);
+        if (!in_bulk) h[r++] = make_int2(y, z);
       }
-    if (bulk)
-      for (long r0 = 0; r0 < (long)ry * rz; r0 += 32) eo[ne++] = make_int2(k, (int)r0);
-    if (d->nx > b->max_nx) b->max_nx = d->nx;
+    const long rows = r - r0;
+    for (long j = 0; j < (rows * (d->nx - 4) + 127) / 128; ++j) rb[ir++] = make_int4(k, (int)r0, (int)rows, (int)j);
+    if (bulk && lp)
+      for (long q = 0; q < (long)ry * rz; q += 32) eo[ie++] = make_int2(k, (int)q);
+    if (bulk && !lp)
+      for (long j = 0; j < ((long)ry * rz * ((d->nx - 4) / 2) + 127) / 128; ++j) xo[ix++] = make_int2(k, (int)j);
   }
-  b->nrows = r;
+  b->nrblk = nr;
   b->neblk = ne;
+  b->nxblk = nxb;
   int rc = 0;
-  if (cudaMalloc(&b->rows, sizeof(int4) * (r ? r : 1)) != cudaSuccess) rc = -5;
-  else if (r && cudaMemcpy(b->rows, h, sizeof(int4) * r, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
+  if (cudaMalloc(&b->rowyz, sizeof(int2) * (n ? n : 1)) != cudaSuccess) rc = -5;
+  else if (n && cudaMemcpy(b->rowyz, h, sizeof(int2) * n, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
+  if (!rc && cudaMalloc(&b->rblk, sizeof(int4) * (nr ? nr : 1)) != cudaSuccess) rc = -5;
+  else if (!rc && nr && cudaMemcpy(b->rblk, rb, sizeof(int4) * nr, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
   if (!rc && cudaMalloc(&b->eblk, sizeof(int2) * (ne ? ne : 1)) != cudaSuccess) rc = -5;
   else if (!rc && ne && cudaMemcpy(b->eblk, eo, sizeof(int2) * ne, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
+  if (!rc && cudaMalloc(&b->xblk, sizeof(int2) * (nxb ? nxb : 1)) != cudaSuccess) rc = -5;
+  else if (!rc && nxb && cudaMemcpy(b->xblk, xo, sizeof(int2) * nxb, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
   free(h);
+  free(rb);
   free(eo);
+  free(xo);
   return rc;
 }
 
@@ -340,9 +382,11 @@ BatchFluid fluid_args(lbib_batch* b, int par, const void* P, const void* WP, int
   f.P = P;
   f.WP = WP;
   f.desc = b->desc;
-  f.rows = b->rows;
-  f.nrows = b->nrows;
-  f.max_nx = b->max_nx;
+  f.rowyz = b->rowyz;
+  f.rblk = b->rblk;
+  f.nrblk = b->nrblk;
+  f.xblk = b->xblk;
+  f.nxblk = b->nxblk;
   f.eblk = b->eblk;
   f.neblk = b->neblk;
   f.list = b->tile_list[c];
@@ -395,10 +439,10 @@ int batch_step(lbib_batch* b) {
         b->launches++;
       }
     if (batch_fluid_rest_lp(f)) return -2;
-    b->launches += 3;
+    b->launches += 1 + (b->nrblk > 0) + (b->neblk > 0);
   } else {
     if (batch_fluid_rest_f64(f)) return -2;
-    b->launches++;
+    b->launches += (b->nxblk > 0) + (b->nrblk > 0);
   }
   /* moments of the touched tiles, read by the next step and the move */
   BatchFluid g = fluid_args(b, par ^ 1, b->P[c], b->WP[c], c);
@@ -520,7 +564,7 @@ lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision
     D.sc2 = p->Ks_l / (D.ds2 * D.ds2);
     D.dt = 1.0;
     int ry = 0, rz = 0;
-    D.bulk = t != LBIB_PREC_F64 && lbdev_bulk_rows(d, &ry, &rz) ? 1 : 0;
+    D.bulk = lbdev_bulk_rows(d, &ry, &rz) ? 1 : 0;
     b->cells += d->N;
     foff = align_up(foff, 256);
     d->f = (void*)foff;                /* offsets for now, pointers below */
@@ -676,7 +720,7 @@ void lbib_batch_free(lbib_batch* b) {
   cudaFree(b->err);
   cudaFree(b->step_no);
   if (b->h_err) cudaFreeHost(b->h_err);
-  cudaFree(b->desc); cudaFree(b->rows); cudaFree(b->eblk);
+  cudaFree(b->desc); cudaFree(b->rowyz); cudaFree(b->rblk); cudaFree(b->eblk); cudaFree(b->xblk);
   for (int v = 0; v < MAXV; ++v) cudaFree(b->wblk[v]);
   if (b->stream) cudaStreamDestroy(b->stream);
   free(b->prob); free(b->h_desc); free(b->variant);

@@ -7,16 +7,18 @@
  * the batch's pools); its tiles are a slice [tile0, tile0 + ntiles) of one
  * global tile space, so one touched-tile list, one slot space and one
  * compaction serve the whole batch.  Work is enumerated across problems:
- *   rows     (problem, y, z) of the rows the generic kernel takes;
+ *   rows     blocks of 128 cells over the rows the generic kernel takes,
+ *            each problem's rows laid end to end;
+ *   pairs    (FP64) blocks of 128 cell pairs of the two-cell kernel;
  *   words    blocks of the word kernel, (problem, block within problem);
- *   edges    the cells x in {2, 3, nx-4, nx-3} of bulk rows, blocks of
- *            (problem, 32 rows);
+ *   edges    (low precision) the cells x in {2, 3, nx-4, nx-3} of bulk
+ *            rows, blocks of (problem, 32 rows);
  *   tiles    the global touched-tile list, tile -> problem by a table.
  * A problem whose error word is set (a fiber stencil left its grid) is
  * skipped by every kernel from then on; the others continue.
  *
- * The per-cell arithmetic is the one-grid code (step_cell, words_item,
- * tile_moments_cell), so a problem advanced in a batch gets the same
+ * The per-cell arithmetic is the one-grid code (step_cell, x2_pair,
+ * words_item, tile_moments_cell), so a problem advanced in a batch gets the same
  * numbers as the same problem on its own.
  */
 #ifndef LBIB_BATCH_CUH
@@ -47,17 +49,23 @@ __device__ __forceinline__ void block_copy(S& dst, const S* __restrict__ src) {
   __syncthreads();
 }
 
-/* Generic rows: one block per (problem, y, z) row and 128 x cells. */
+/* Generic rows: a block per 128 cells of a problem's rows, the rows of
+ * problem k laid end to end (cell c of the item: row c / (nx-4), x = 2 +
+ * c % (nx-4)), so small grids fill their blocks.  Item m = (problem, first
+ * row in rowyz, rows of the problem, chunk). */
 template <typename T, int PAR>
-__global__ void __launch_bounds__(128) lbib_b_rows(const FluidParamsT<T>* __restrict__ P, const int4* __restrict__ rows,
-                                                   const int* __restrict__ err) {
+__global__ void __launch_bounds__(128) lbib_b_rows(const FluidParamsT<T>* __restrict__ P, const int2* __restrict__ rowyz,
+                                                   const int4* __restrict__ rblk, const int* __restrict__ err) {
   __shared__ __align__(16) FluidParamsT<T> sp;
-  const int4 r = rows[blockIdx.x];
-  if (err[2 * r.x]) return;
-  block_copy(sp, P + r.x);
-  const int x = blockIdx.y * blockDim.x + threadIdx.x + 2;
-  if (x > sp.nx - 3) return;
-  step_cell<T, PAR>(sp, x, r.y, r.z);
+  const int4 m = rblk[blockIdx.x];
+  if (err[2 * m.x]) return;
+  block_copy(sp, P + m.x);
+  const int w = sp.nx - 4;
+  const int c = m.w * 128 + threadIdx.x;
+  const int r = c / w;
+  if (r >= m.z) return;
+  const int2 yz = rowyz[m.y + r];
+  step_cell<T, PAR>(sp, 2 + c % w, yz.x, yz.y);
 }
 
 /* Word kernel over the blocks of all problems that run it. */

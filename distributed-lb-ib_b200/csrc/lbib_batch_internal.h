@@ -21,9 +21,11 @@ struct BatchFluid {
   const void* P;           /* FluidParamsT<T>[B] */
   const void* WP;          /* WordsParams<T>[B] */
   const BatchDesc* desc;
-  const int4* rows;        /* generic rows */
-  long nrows;
-  int max_nx;
+  const int2* rowyz;       /* generic rows (y, z), each problem's contiguous */
+  const int4* rblk;        /* generic-row blocks: (problem, first row, rows, chunk) */
+  long nrblk;
+  const int2* xblk;        /* FP64 two-cell blocks: (problem, block) */
+  long nxblk;
   const int2* eblk;        /* edge-cell blocks: (problem, first bulk row) */
   long neblk;
   const int* list;         /* touched tiles (global ids) */
@@ -35,7 +37,8 @@ struct BatchFluid {
   int grid_tiles;          /* persistent grid for tile-list kernels */
 };
 
-/* Generic rows + edge cells + forced cells (the word blocks are separate). */
+/* Generic rows + edge cells + forced cells (the word blocks are separate);
+ * FP64: two-cell blocks + generic rows. */
 int batch_fluid_rest_f64(const BatchFluid& f);
 int batch_fluid_rest_lp(const BatchFluid& f);
 /* Word-kernel blocks of one variant. */

@@ -14,10 +14,9 @@ template <typename T>
 int rest(const BatchFluid& f) {
   const FluidParamsT<T>* P = static_cast<const FluidParamsT<T>*>(f.P);
   const WordsParams<T>* WP = static_cast<const WordsParams<T>*>(f.WP);
-  if (f.nrows > 0) {
-    dim3 grid((unsigned)f.nrows, (unsigned)((f.max_nx - 4 + 127) / 128));
-    if (f.par == 0) lbib_b_rows<T, 0><<<grid, 128, 0, f.stream>>>(P, f.rows, f.err);
-    else lbib_b_rows<T, 1><<<grid, 128, 0, f.stream>>>(P, f.rows, f.err);
+  if (f.nrblk > 0) {
+    if (f.par == 0) lbib_b_rows<T, 0><<<(unsigned)f.nrblk, 128, 0, f.stream>>>(P, f.rowyz, f.rblk, f.err);
+    else lbib_b_rows<T, 1><<<(unsigned)f.nrblk, 128, 0, f.stream>>>(P, f.rowyz, f.rblk, f.err);
   }
   if (f.neblk > 0) {
     if (f.par == 0) lbib_b_edges<T, 0><<<(unsigned)f.neblk, 128, 0, f.stream>>>(P, WP, f.eblk, f.err);

@@ -21,7 +21,8 @@ reaches T.  Both are trained by the library's own GPU kernels (lbib_mlp_*:
 BF16 tensor-core GEMMs, Adam).
 
 Screen: the nets predict every point at t = T.  A point is re-run by the
-plain FP64 solver when its stop output is undecided, when it is among the
+batched solver (FP16 flow-shifted storage by default, FP64 on request) when
+its stop output is undecided, when it is among the
 top 5% of the points predicted to reach T by tip displacement (the points a
 sweep is after), or when the members disagree on its tip by more than a
 threshold; every other point is reported from the surrogate: "stops", or
@@ -244,15 +245,19 @@ def screen(model, problems, top: float = 0.05, disagree: float = 0.01, band: flo
                     "top": int(topk.sum())}}
 
 
-def evaluate(model, problems, steps: int, truth=None, thresholds=None) -> Dict:
-    """Screen `problems`, re-run the flagged ones with the plain FP64 solver,
-    and judge every reported point against the plain solver's own run."""
+def evaluate(model, problems, steps: int, truth=None, thresholds=None, rerun_precision: str = "f16-flow") -> Dict:
+    """Screen `problems`, re-run the flagged ones with the batched solver in
+    `rerun_precision`, and judge every point -- reported or re-run --
+    against the plain FP64 solver's own run."""
     th = thresholds or {}
     s = screen(model, problems, disagree=th.get("disagree", 0.01), band=th.get("stop_band", 0.3))
     idx = np.nonzero(s["rerun"])[0]
+    tip, goes = s["tip"].copy(), s["alive"].copy()
     rerun_s = 0.0
     if len(idx):
-        d, a, _, rerun_s = simulate([problems[i] for i in idx], steps, steps, "f64")
+        d, a, _, rerun_s = simulate([problems[i] for i in idx], steps, steps, rerun_precision)
+        d, a = clean(d, a)
+        tip[idx], goes[idx] = tip_of(d[:, -1]), a[:, -1]
     if truth is None:
         truth = simulate(problems, steps, steps, "f64")
     tdisp, talive, _, plain_s = truth
@@ -260,17 +265,22 @@ def evaluate(model, problems, steps: int, truth=None, thresholds=None) -> Dict:
     true_tip = tip_of(tdisp[:, -1])
     true_alive = talive[:, -1]
     rep = ~s["rerun"]
-    # a reported point is right when it gets "stopped" right, and, for a run
-    # that completes, its tip within 2% (or 0.02 lattice units for tiny tips)
-    tip_ok = np.abs(s["tip"] - true_tip) <= np.maximum(0.02 * np.abs(true_tip), 0.02)
+    # a point is right when it gets "stopped" right, and, for a run that
+    # completes, its tip within 2% (or 0.02 lattice units for tiny tips)
+    tip_ok = np.abs(tip - true_tip) <= np.maximum(0.02 * np.abs(true_tip), 0.02)
     rel = np.abs(s["tip"] - true_tip) / np.maximum(np.abs(true_tip), 1e-3)
-    right = (s["alive"] == true_alive) & (~true_alive | tip_ok)
+    right = (goes == true_alive) & (~true_alive | tip_ok)
+    rr = s["rerun"]
     sur_s = s["seconds"] + rerun_s
     return {"points": len(problems), "reported_by_surrogate": int(rep.sum()), "rerun": int(len(idx)), "rerun_why": s["why"],
+            "rerun_precision": rerun_precision, "rerun_s": rerun_s, "screen_s": s["seconds"],
             "plain_fp64_s": plain_s, "plain_points_per_s": len(problems) / plain_s,
             "surrogate_s": sur_s, "surrogate_points_per_s": len(problems) / sur_s,
             "speedup": plain_s / sur_s,
+            "right": int(right.sum()), "right_frac": float(right.mean()),
             "reported_right": int(right[rep].sum()), "reported_right_frac": float(right[rep].mean()) if rep.any() else 1.0,
+            "rerun_right": int(right[rr].sum()),
+            "completed": int(true_alive.sum()), "completed_tip_within_2pct": int((true_alive & tip_ok & (goes == true_alive)).sum()),
             "reported_completed": int((rep & true_alive).sum()),
             "reported_completed_tip_within_2pct": int((rep & true_alive & tip_ok).sum()),
             "stop_prediction_accuracy": float((s["alive"] == true_alive).mean()),
@@ -289,6 +299,8 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--iters", type=int, default=10000)
+    ap.add_argument("--rerun-precision", default="f16-flow",
+                    help="storage of the batched solver that re-runs the flagged points (f64: the plain solver)")
     ap.add_argument("--data", default=None,
                     help="directory to keep the simulated runs in (reused when present: only the "
                          "training and the screen run again)")
@@ -325,7 +337,8 @@ def main(argv=None) -> int:
         truth = simulate(ev, a.steps, a.steps, "f64")
         if fev:
             np.savez(fev, disp=truth[0], alive=truth[1], stop=truth[2], seconds=truth[3])
-    out["evaluation"] = evaluate(model, ev, a.steps, truth=truth, thresholds=th)
+    out["evaluation"] = evaluate(model, ev, a.steps, truth=truth, thresholds=th,
+                                 rerun_precision=a.rerun_precision)
     for n in model[0] + [model[1]]:
         n.close()
     print(json.dumps(out))

@@ -1,6 +1,6 @@
 """The learned sweep screen end to end, at a small size: batched runs make
-the training set, the GPU MLP learns it, and the screen's reported points
-are judged against the plain FP64 solver.  The trained network must beat
+the training set, the GPU MLP learns it, and every point of the screen (reported
+or re-run) is judged against the plain FP64 solver.  The trained network must beat
 the same network untrained on the held-out points (what training gains),
 and the screen must be cheaper than running every point."""
 import numpy as np
@@ -36,7 +36,11 @@ def test_surrogate_learns_and_screens(gpu):
     assert err_trained < 0.5 * err_untrained, (err_trained, err_untrained)
     rep = surrogate.evaluate(model, ev, steps, truth=truth)
     assert rep["points"] == 32 and rep["rerun"] + rep["reported_by_surrogate"] == 32
-    assert rep["rerun"] >= 2                      # the top 5% always go to the plain solver
+    assert rep["rerun"] >= 2                      # the top 5% always go to the solver
     assert 0.0 <= rep["reported_right_frac"] <= 1.0
+    assert rep["rerun_right"] >= 0.9 * rep["rerun"]          # FP16 re-runs judged by FP64
+    rep64 = surrogate.evaluate(model, ev, steps, truth=truth, rerun_precision="f64")
+    assert rep64["rerun"] == rep["rerun"]
+    assert rep64["rerun_right"] == rep64["rerun"]           # the plain solver is its own judge
     for n in model[0] + [model[1]] + untrained[0] + [untrained[1]]:
         n.close()
