@@ -83,6 +83,7 @@ void init_gv_constant(GV gv) {
   memcpy(gv->c, LBIB_C, sizeof(LBIB_C));
   gv->lbib_compat = LBIB_COMPAT_ALL;
   gv->lbib_precision = LBIB_PREC_F64;
+  gv->lbib_slab_lo = gv->lbib_slab_hi = 0;
 }
 
 static void fill_config(GV gv, lbdev_config* c) {
@@ -95,6 +96,7 @@ static void fill_config(GV gv, lbdev_config* c) {
   c->tau = gv->tau; c->u_l = gv->u_l; c->rho_l = gv->rho_l;
   c->Ks_l = gv->Ks_l; c->Kb_l = gv->Kb_l; c->g_l = gv->g_l; c->cs_l = gv->cs_l;
   c->dt = gv->dt;
+  c->x_lo = gv->lbib_slab_lo; c->x_hi = gv->lbib_slab_hi;
 }
 
 void gen_fluid_grid(Fluidgrid* fluid_grid, int cube_size, int taskid, GV gv) {
@@ -265,6 +267,83 @@ int lbib_set_precision(GV gv, int precision) {
   return LBIB_OK;
 }
 
+int lbib_set_slab(GV gv, int x_lo, int x_hi) {
+  if (!gv) return set_error(LBIB_E_ARG);
+  if (gv->dev && gv->dev->S > 0) return set_error(LBIB_E_STATE);
+  const int keep_lo = gv->lbib_slab_lo, keep_hi = gv->lbib_slab_hi;
+  gv->lbib_slab_lo = x_lo;
+  gv->lbib_slab_hi = x_hi;
+  if (gv->dev) {
+    lbdev_free(gv->dev);
+    gv->dev = NULL;
+    lbdev_config c;
+    fill_config(gv, &c);
+    int rc = lbdev_create(&gv->dev, &c);
+    if (rc) {
+      gv->lbib_slab_lo = keep_lo;
+      gv->lbib_slab_hi = keep_hi;
+      fill_config(gv, &c);
+      lbdev_create(&gv->dev, &c);
+      return set_error(rc);
+    }
+  }
+  return LBIB_OK;
+}
+
+static int is_slab(GV gv) { return gv->dev && (gv->dev->x_lo > 0 || gv->dev->x_hi < gv->dev->nx); }
+
+int lbib_slab_buffers(GV gv, double** bufs, long* len) {
+  if (!gv || !bufs || !len) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv)) return set_error(LBIB_E_STATE);
+  const long P5 = 5L * gv->dev->ny * gv->dev->nz;
+  for (int k = 0; k < 4; ++k) bufs[k] = gv->dev->halo + k * P5;
+  *len = P5;
+  return LBIB_OK;
+}
+
+int lbib_slab_step_fluid(GV gv) {
+  if (!gv) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv)) return set_error(LBIB_E_STATE);
+  lbib_device* d = gv->dev;
+  static const int order[] = {0, 3, 4};
+  for (int i = 0; i < 3; ++i) {
+    int rc = lbdev_stage(d, order[i], gv->time);
+    if (rc) return set_error(rc);
+  }
+  const int par = d->parity ^ 1;      /* the step just launched */
+  if (lbdev_slab_pack(d, par)) return set_error(LBIB_E_CUDA);
+  return par;
+}
+
+int lbib_slab_step_moments(GV gv) {
+  if (!gv) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv) || gv->dev->steps == 0) return set_error(LBIB_E_STATE);
+  if (lbdev_slab_unpack(gv->dev, gv->dev->parity ^ 1)) return set_error(LBIB_E_CUDA);
+  int rc = lbdev_stage(gv->dev, 7, gv->time);
+  return rc ? set_error(rc) : LBIB_OK;
+}
+
+int lbib_slab_moments(GV gv, double** U, long* n) {
+  if (!gv || !U || !n) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv) || !gv->dev->have_moments) return set_error(LBIB_E_STATE);
+  int failed = 0;
+  int e = lbdev_slab_moments(gv->dev, U, n, &failed);
+  if (e) {
+    if (e != LBIB_E_CUDA) gv->time = failed;
+    return set_error(e);
+  }
+  return LBIB_OK;
+}
+
+int lbib_slab_step_move(GV gv) {
+  if (!gv) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv)) return set_error(LBIB_E_STATE);
+  int rc = lbdev_stage(gv->dev, 8, gv->time);
+  if (rc) return set_error(rc);
+  gv->time += gv->dt;
+  return LBIB_OK;
+}
+
 int lbib_kernel_variants(GV gv) {
   if (!gv || !gv->dev) return set_error(LBIB_E_STATE);
   return lbdev_variants(gv->dev);
@@ -290,6 +369,7 @@ int lbib_autotune(GV gv, int steps, double* ms_per_variant, int max_variants) {
 
 int lbib_save_restart(GV gv, const char* path) {
   if (!gv || !gv->dev || !gv->fiber_shape || !path) return set_error(LBIB_E_STATE);
+  if (is_slab(gv)) return set_error(LBIB_E_STATE);
   FILE* fp = fopen(path, "wb");
   if (!fp) return set_error(LBIB_E_IO);
   lbib_device* d = gv->dev;
@@ -308,6 +388,7 @@ int lbib_save_restart(GV gv, const char* path) {
 
 int lbib_load_restart(GV gv, const char* path) {
   if (!gv || !gv->dev || !gv->fiber_shape || !path) return set_error(LBIB_E_STATE);
+  if (is_slab(gv)) return set_error(LBIB_E_STATE);
   FILE* fp = fopen(path, "rb");
   if (!fp) return set_error(LBIB_E_IO);
   lbib_device* d = gv->dev;
@@ -453,6 +534,7 @@ void* do_thread(void* v) {
 
 int lbib_run(GV gv, int nsteps) {
   if (!gv || nsteps < 0) return set_error(LBIB_E_ARG);
+  if (is_slab(gv)) return set_error(LBIB_E_STATE);
   int keep_ts = gv->timesteps;
   gv->timesteps = gv->time + nsteps - 1;
   struct lv_t lv = {0, gv};
@@ -572,12 +654,39 @@ GV lbib_case_create(int nx, int ny, int nz, int cube_size, int nsheets,
                                tau, u_l, Ks_l, Kb_l, compat, LBIB_PREC_F64);
 }
 
+static GV case_create(int nx, int ny, int nz, int cube_size, int nsheets,
+                      const int* rows, const int* cols,
+                      const double* width, const double* height,
+                      const double* x0, const double* y0, const double* z0,
+                      double tau, double u_l, double Ks_l, double Kb_l, int compat,
+                      int precision, int x_lo, int x_hi);
+
 GV lbib_case_create_prec(int nx, int ny, int nz, int cube_size, int nsheets,
                          const int* rows, const int* cols,
                          const double* width, const double* height,
                          const double* x0, const double* y0, const double* z0,
                          double tau, double u_l, double Ks_l, double Kb_l, int compat,
                          int precision) {
+  return case_create(nx, ny, nz, cube_size, nsheets, rows, cols, width, height, x0, y0, z0,
+                     tau, u_l, Ks_l, Kb_l, compat, precision, 0, 0);
+}
+
+GV lbib_case_create_slab(int nx, int ny, int nz, int cube_size, int nsheets,
+                         const int* rows, const int* cols,
+                         const double* width, const double* height,
+                         const double* x0, const double* y0, const double* z0,
+                         double tau, double u_l, double Ks_l, double Kb_l, int compat,
+                         int x_lo, int x_hi) {
+  return case_create(nx, ny, nz, cube_size, nsheets, rows, cols, width, height, x0, y0, z0,
+                     tau, u_l, Ks_l, Kb_l, compat, LBIB_PREC_F64, x_lo, x_hi);
+}
+
+static GV case_create(int nx, int ny, int nz, int cube_size, int nsheets,
+                      const int* rows, const int* cols,
+                      const double* width, const double* height,
+                      const double* x0, const double* y0, const double* z0,
+                      double tau, double u_l, double Ks_l, double Kb_l, int compat,
+                      int precision, int x_lo, int x_hi) {
   if (nsheets < 1 || !rows || !cols || !width || !height || !x0 || !y0 || !z0 ||
       !precision_ok(precision)) {
     set_error(LBIB_E_ARG);
@@ -602,6 +711,8 @@ GV lbib_case_create_prec(int nx, int ny, int nz, int cube_size, int nsheets,
   init_gv_constant(gv);
   gv->lbib_compat = compat;
   gv->lbib_precision = precision;
+  gv->lbib_slab_lo = x_lo;
+  gv->lbib_slab_hi = x_hi;
   gv->tau = tau; gv->u_l = u_l; gv->Ks_l = Ks_l; gv->Kb_l = Kb_l;
   gen_fluid_grid(gv->fluid_grid, cube_size, 0, gv);
   for (int k = 0; k < nsheets; ++k) gen_fiber_sheet(&gv->fiber_shape->sheets[k]);

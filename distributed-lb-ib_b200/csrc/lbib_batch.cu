@@ -145,12 +145,12 @@ __global__ void __launch_bounds__(128, 3) lbib_b_x2(const FluidParams* __restric
   const int2 m = blk[blockIdx.x];
   if (err[2 * m.x]) return;
   block_copy(sp, P + m.x);
-  const int npairs = (sp.nx - 4) / 2, nry = sp.ny - 6;
+  const int npairs = (sp.xhi - sp.xlo + 1) / 2, nry = sp.ny - 6;
   const long g = (long)m.y * 128 + threadIdx.x;
   const long row = g / npairs;
   if (row >= (long)nry * x2_rows_z(sp.nz, sp.zin_hi)) return;
   const int pr = (int)(g - row * npairs);
-  x2_pair<PAR>(sp, 2 + 2 * pr, 3 + (int)(row % nry), 3 + (int)(row / nry));
+  x2_pair<PAR>(sp, sp.xlo + 2 * pr, 3 + (int)(row % nry), 3 + (int)(row / nry));
 }
 
 template <int PAR>
@@ -544,6 +544,7 @@ lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision
     b->sh[k] = d;
     d->nx = p->nx; d->ny = p->ny; d->nz = p->nz; d->prec = precision;
     d->N = (long)p->nx * p->ny * p->nz;
+    lbdev_set_columns(d, 0, 0);
     d->cube_size = 4;
     d->ncx = p->nx / 4; d->ncy = p->ny / 4; d->ncz = p->nz / 4;
     lbdev_set_physics(d, &c);          /* constants and boundary rows; no stream yet: no allocation */

@@ -160,6 +160,21 @@ extern "C" int lbdev_set_physics(lbib_device* d, const lbdev_config* c) {
   return d->stream ? build_rows(d) : 0;
 }
 
+/* The columns [x_lo, x_hi) of the global grid this state holds (x_hi <= 0:
+ * all of them).  A slab's bounds are multiples of 4, so every 4^3 tile lies
+ * in one slab, and it is stored with two ghost columns on each side (even,
+ * so the two-cell kernel's 16-byte accesses stay aligned). */
+extern "C" int lbdev_set_columns(lbib_device* d, int x_lo, int x_hi) {
+  if (x_hi <= 0) { x_lo = 0; x_hi = d->nx; }
+  if (x_lo < 0 || x_hi > d->nx || x_hi - x_lo < 4 || x_lo % 4 || x_hi % 4) return -1;
+  const int whole = x_lo == 0 && x_hi == d->nx;
+  d->x_lo = x_lo; d->x_hi = x_hi;
+  d->gx0 = whole ? 0 : x_lo - 2;
+  d->sx = whole ? d->nx : x_hi - x_lo + 4;
+  d->Ns = (long)d->sx * d->ny * d->nz;
+  return 0;
+}
+
 extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   *out = NULL;
   if (c->nx < 8 || c->ny < 8 || c->nz < 8 || c->cube_size < 4) return -1;
@@ -169,6 +184,12 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   d->nx = c->nx; d->ny = c->ny; d->nz = c->nz;
   d->prec = c->prec;
   d->N = (long)c->nx * c->ny * c->nz;
+  /* slabs: FP64 only (the low-precision word kernel addresses whole rows) */
+  if (lbdev_set_columns(d, c->x_lo, c->x_hi) ||
+      ((d->x_lo > 0 || d->x_hi < d->nx) && LBIB_PREC_TYPE(c->prec) != LBIB_PREC_F64)) {
+    free(d);
+    return -1;
+  }
   d->cube_size = c->cube_size;
   d->ncx = c->nx / c->cube_size; d->ncy = c->ny / c->cube_size; d->ncz = c->nz / c->cube_size;
   lbdev_set_physics(d, c);
@@ -178,14 +199,16 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   d->ntiles = (long)d->ntx * d->nty * d->ntz;
   int rc = 0;
   const size_t pop = lbdev_pop_bytes(d->prec), real = LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 ? 8 : 4;
-  if (cudaMalloc(&d->f, pop * 19 * d->N) != cudaSuccess) rc = -5;
+  if (cudaMalloc(&d->f, pop * 19 * d->Ns) != cudaSuccess) rc = -5;
   long P = (long)d->ny * d->nz;
   if (!rc && cudaMalloc(&d->inlet, real * 19 * P) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&d->outlet, real * 19 * P) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&d->err, sizeof(int) * 2) != cudaSuccess) rc = -5;
   if (!rc && cudaMallocHost(&d->h_err, sizeof(int) * 2) != cudaSuccess) rc = -5;
   if (!rc && cudaMemsetAsync(d->err, 0, sizeof(int) * 2, d->stream) != cudaSuccess) rc = -2;
-  if (!rc && cudaMemsetAsync(d->f, 0, pop * 19 * d->N, d->stream) != cudaSuccess) rc = -2;
+  if (!rc && cudaMemsetAsync(d->f, 0, pop * 19 * d->Ns, d->stream) != cudaSuccess) rc = -2;
+  if (!rc && (d->x_lo > 0 || d->x_hi < d->nx) &&
+      cudaMalloc(&d->halo, sizeof(double) * 20 * P) != cudaSuccess) rc = -5;
   if (!rc) rc = build_rows(d);
   if (rc) { lbdev_free(d); return rc; }
   d->cur = 0;
@@ -241,6 +264,7 @@ extern "C" void lbdev_free(lbib_device* d) {
   free_tiles(d);
   free_sheets(d);
   cudaFree(d->f); cudaFree(d->inlet); cudaFree(d->outlet); cudaFree(d->err); cudaFree(d->rows);
+  cudaFree(d->halo);
   cudaFree(d->scratch);
   for (long i = 0; i < 6 * d->prof_cap; ++i) cudaEventDestroy(d->prof_ev[i]);
   free(d->prof_ev);
@@ -557,7 +581,7 @@ extern "C" int lbdev_save_state(lbib_device* d, FILE* fp) {
   if (!buf) return -5;
   const size_t real = LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 ? 8 : 4;
   const long P = (long)d->ny * d->nz;
-  if (!rc) rc = dev_out(d, fp, d->f, lbdev_pop_bytes(d->prec) * 19 * d->N, buf, cap);
+  if (!rc) rc = dev_out(d, fp, d->f, lbdev_pop_bytes(d->prec) * 19 * d->Ns, buf, cap);
   if (!rc) rc = dev_out(d, fp, d->inlet, real * 19 * P, buf, cap);
   if (!rc) rc = dev_out(d, fp, d->outlet, real * 19 * P, buf, cap);
   if (!rc) rc = dev_out(d, fp, d->tile_slot[c], sizeof(int) * d->ntiles, buf, cap);
@@ -582,7 +606,7 @@ extern "C" int lbdev_load_state(lbib_device* d, FILE* fp) {
   if (!buf) return -5;
   const size_t real = LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 ? 8 : 4;
   const long P = (long)d->ny * d->nz;
-  int rc = dev_in(d, fp, d->f, lbdev_pop_bytes(d->prec) * 19 * d->N, buf, cap);
+  int rc = dev_in(d, fp, d->f, lbdev_pop_bytes(d->prec) * 19 * d->Ns, buf, cap);
   if (!rc) rc = dev_in(d, fp, d->inlet, real * 19 * P, buf, cap);
   if (!rc) rc = dev_in(d, fp, d->outlet, real * 19 * P, buf, cap);
   if (!rc) rc = dev_in(d, fp, d->tile_slot[c], sizeof(int) * d->ntiles, buf, cap);

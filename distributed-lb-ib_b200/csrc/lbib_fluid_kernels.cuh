@@ -199,7 +199,7 @@ struct Form<T, true> {
 template <typename T, int PAR>
 __device__ __forceinline__ void step_cell(const FluidParamsT<T>& p, int x, int y, int z) {
   using R = typename Pop<T>::R;
-  const long idx = ((long)z * p.ny + y) * p.nx + x;
+  const long idx = sidx(p, x, y, z);
   const int kind = classify(p, x, y, z);
   R f[19];
   load_pre<PAR>(p, x, y, z, idx, kind, f);
@@ -227,15 +227,17 @@ __device__ __forceinline__ void step_cell(const FluidParamsT<T>& p, int x, int y
 template <typename T, int PAR>
 __global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
     lbib_fluid_step(FluidParamsT<T> p, const int2* __restrict__ rows) {
-  const int x = blockIdx.y * blockDim.x + threadIdx.x + 2;
+  const int x = blockIdx.y * blockDim.x + threadIdx.x + p.xlo;
   const int2 r = rows[blockIdx.x];
-  if (x > p.nx - 3) return;
+  if (x > p.xhi) return;
   step_cell<T, PAR>(p, x, r.x, r.y);
 }
 
 /* (rho, u)(t) of every cell of the touched tiles, after the fused step of
  * parity 1-PAR: compute_rho_and_u (lbm_ib.c:2440-2538) restricted to where
- * moveFiberSheet will read.  Cells outside M keep the initial values. */
+ * moveFiberSheet will read.  Cells outside M keep the initial values.  A
+ * tile outside this state's columns gets -0.0, the identity of a sum, so
+ * that adding the tiles of all slabs gives every value with its bits. */
 template <typename T, int PAR>
 __device__ __forceinline__ void tile_moments_cell(const FluidParamsT<T>& p, int tile, int i, int cell,
                                                   const double* __restrict__ Ftile, double* __restrict__ Utile) {
@@ -244,8 +246,10 @@ __device__ __forceinline__ void tile_moments_cell(const FluidParamsT<T>& p, int 
     const int tx = tile % p.ntx, ty = (tile / p.ntx) % p.nty, tz = tile / (p.ntx * p.nty);
     const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
     double rho = p.rho0, ux = p.ux0, uy = 0.0, uz = 0.0;
-    if (x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
-      const long idx = ((long)z * p.ny + y) * p.nx + x;
+    if (tx * 4 < p.olo || tx * 4 >= p.ohi) {
+      rho = ux = uy = uz = -0.0;
+    } else if (x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
+      const long idx = sidx(p, x, y, z);
       R f[19];
       load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
       const double* Ft = Ftile + (long)i * 192;
@@ -266,18 +270,19 @@ __global__ void lbib_tile_moments(FluidParamsT<T> p, const int* __restrict__ lis
   for (int i = blockIdx.x; i < n; i += gridDim.x) tile_moments_cell<T, PAR>(p, list[i], i, threadIdx.x, Ftile, Utile);
 }
 
-/* Dense rho, u over the whole grid as the reference holds them after the
- * step: M cells from the populations (with this step's force where a tile
- * carried one), all other cells at the initial values. */
+/* Dense rho, u over the grid as the reference holds them after the step:
+ * M cells from the populations (with this step's force where a tile carried
+ * one), all other cells at the initial values; this state's columns only,
+ * written at their global index. */
 template <typename T, int PAR>
 __global__ void lbib_field_moments(FluidParamsT<T> p, int have_step, double* __restrict__ rho_o,
                                    double* __restrict__ ux_o, double* __restrict__ uy_o,
                                    double* __restrict__ uz_o) {
   using R = typename Pop<T>::R;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + p.olo;
   const int y = blockIdx.y, z = blockIdx.z;
-  if (x >= p.nx) return;
-  const long idx = ((long)z * p.ny + y) * p.nx + x;
+  if (x >= p.ohi) return;
+  const long idx = sidx(p, x, y, z);
   double rho = p.rho0, ux = p.ux0, uy = 0.0, uz = 0.0;
   if (have_step && x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
     R f[19];
@@ -293,22 +298,25 @@ __global__ void lbib_field_moments(FluidParamsT<T> p, int have_step, double* __r
     Form<T>::moments(f, Fx, Fy, Fz, p, m);
     Form<T>::to_double(m, p, rho, ux, uy, uz);
   }
-  rho_o[idx] = rho; ux_o[idx] = ux; uy_o[idx] = uy; uz_o[idx] = uz;
+  const long g = ((long)z * p.ny + y) * p.nx + x;
+  rho_o[g] = rho; ux_o[g] = ux; uy_o[g] = uy; uz_o[g] = uz;
 }
 
-/* df1 as the reference holds it at the start of the next step, for cells of
- * I (natural layout [q][idx]); other cells are left untouched. */
+/* df1 as the reference holds it at the start of the next step, for this
+ * state's cells of I (natural layout [q][idx] of the global grid); other
+ * cells are left untouched. */
 template <typename T, int PAR>
 __global__ void lbib_gather_df1(FluidParamsT<T> p, double* __restrict__ out) {
   using R = typename Pop<T>::R;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + p.xlo;
   const int y = blockIdx.y + 2, z = blockIdx.z + 2;
-  if (x > p.nx - 3) return;
-  const long idx = ((long)z * p.ny + y) * p.nx + x;
+  if (x > p.xhi) return;
+  const long idx = sidx(p, x, y, z);
   R f[19];
   load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
+  const long G = (long)p.nx * p.ny * p.nz, g = ((long)z * p.ny + y) * p.nx + x;
 #pragma unroll
-  for (int q = 0; q < 19; ++q) out[q * p.N + idx] = Form<T>::value(f[q], q, p);
+  for (int q = 0; q < 19; ++q) out[q * G + g] = Form<T>::value(f[q], q, p);
 }
 
 /* FP64 mass and momentum of the populations of I as the next step reads
@@ -320,8 +328,8 @@ __global__ void __launch_bounds__(128) lbib_row_sums(FluidParamsT<T> p, double* 
   using R = typename Pop<T>::R;
   const int y = blockIdx.x + 2, z = blockIdx.y + 2;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-  for (int x = threadIdx.x + 2; x <= p.nx - 3; x += blockDim.x) {
-    const long idx = ((long)z * p.ny + y) * p.nx + x;
+  for (int x = threadIdx.x + p.xlo; x <= p.xhi; x += blockDim.x) {
+    const long idx = sidx(p, x, y, z);
     R f[19];
     load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
     double m = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
@@ -386,7 +394,10 @@ FluidParamsT<T> make_params_t(lbib_device* d, int first) {
   using R = typename Pop<T>::R;
   FluidParamsT<T> p;
   p.f = (T*)d->f; p.inlet = (const R*)d->inlet; p.outlet = (const R*)d->outlet;
-  p.N = d->N; p.nx = d->nx; p.ny = d->ny; p.nz = d->nz;
+  p.N = d->Ns; p.nx = d->nx; p.ny = d->ny; p.nz = d->nz;
+  p.sx = d->sx; p.gx0 = d->gx0; p.olo = d->x_lo; p.ohi = d->x_hi;
+  p.xlo = d->x_lo > 2 ? d->x_lo : 2;
+  p.xhi = d->x_hi - 1 < d->nx - 3 ? d->x_hi - 1 : d->nx - 3;
   p.zin_hi = d->zin_hi; p.yskip_z0 = d->yskip_z0; p.first = first;
   p.rho0 = d->rho_l; p.ux0 = d->u_l;
   p.omtau = d->omtau; p.invtau = d->invtau;
@@ -414,7 +425,7 @@ template <typename T>
 int launch_step_rows_t(lbib_device* d, const FluidParamsT<T>& p) {
   if (d->nrows <= 0) return 0;
   dim3 block(128);
-  dim3 grid((unsigned)d->nrows, (unsigned)((d->nx - 4 + 127) / 128));
+  dim3 grid((unsigned)d->nrows, (unsigned)((p.xhi - p.xlo + 1 + 127) / 128));
   if (d->parity == 0) lbib_fluid_step<T, 0><<<grid, block, 0, d->stream>>>(p, (const int2*)d->rows);
   else lbib_fluid_step<T, 1><<<grid, block, 0, d->stream>>>(p, (const int2*)d->rows);
   d->kernel_launches++;
@@ -438,7 +449,7 @@ template <typename T>
 int launch_field_moments_t(lbib_device* d, double* rho, double* ux, double* uy, double* uz) {
   FluidParamsT<T> p = make_params_t<T>(d, 0);
   dim3 block(128);
-  dim3 grid((unsigned)((d->nx + 127) / 128), (unsigned)d->ny, (unsigned)d->nz);
+  dim3 grid((unsigned)((p.ohi - p.olo + 127) / 128), (unsigned)d->ny, (unsigned)d->nz);
   const int have = d->steps > 0 && d->have_forces;
   if (d->parity == 0) lbib_field_moments<T, 0><<<grid, block, 0, d->stream>>>(p, have, rho, ux, uy, uz);
   else lbib_field_moments<T, 1><<<grid, block, 0, d->stream>>>(p, have, rho, ux, uy, uz);
@@ -450,7 +461,7 @@ template <typename T>
 int launch_gather_df1_t(lbib_device* d, double* out) {
   FluidParamsT<T> p = make_params_t<T>(d, d->steps == 0);
   dim3 block(128);
-  dim3 grid((unsigned)((d->nx - 4 + 127) / 128), (unsigned)(d->ny - 4), (unsigned)(d->nz - 4));
+  dim3 grid((unsigned)((p.xhi - p.xlo + 1 + 127) / 128), (unsigned)(d->ny - 4), (unsigned)(d->nz - 4));
   if (d->parity == 0) lbib_gather_df1<T, 0><<<grid, block, 0, d->stream>>>(p, out);
   else lbib_gather_df1<T, 1><<<grid, block, 0, d->stream>>>(p, out);
   d->kernel_launches++;
@@ -476,7 +487,7 @@ int launch_init_t(lbib_device* d, int what) {
   FluidParamsT<T> p = make_params_t<T>(d, 1);
   const int block = 256;
   if (what == 0) {
-    lbib_init_pop<T><<<(unsigned)((d->N + block - 1) / block), block, 0, d->stream>>>(p, (T*)d->f, d->N);
+    lbib_init_pop<T><<<(unsigned)((d->Ns + block - 1) / block), block, 0, d->stream>>>(p, (T*)d->f, d->Ns);
   } else {
     const long P = (long)d->ny * d->nz;
     lbib_init_table<T><<<(unsigned)((P + block - 1) / block), block, 0, d->stream>>>(p, (R*)d->inlet, P);

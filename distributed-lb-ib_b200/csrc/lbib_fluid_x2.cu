@@ -20,7 +20,7 @@ constexpr int TPB = 128;
 struct X2Params {
   FluidParams p;
   int nry;       /* interior rows in y: ny - 6 */
-  int npairs;    /* pairs per row: (nx - 4) / 2 */
+  int npairs;    /* pairs per row: (xhi - xlo + 1) / 2 */
 };
 
 template <int PAR>
@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(TPB, LBIB_X2_MINB) lbib_fluid_step_x2(X2Params
   if (pr >= b.npairs) return;
   const int y = 3 + (int)(blockIdx.x % b.nry);
   const int z = 3 + (int)(blockIdx.x / b.nry);
-  x2_pair<PAR>(b.p, 2 + 2 * pr, y, z);
+  x2_pair<PAR>(b.p, b.p.xlo + 2 * pr, y, z);
 }
 
 }  // namespace
@@ -49,7 +49,7 @@ extern "C" int lbdev_launch_fluid_bulk(lbib_device* d, const void* fluid_params)
   b.p = *(const FluidParams*)fluid_params;
   int nrz = 0;
   if (!lbdev_bulk_rows(d, &b.nry, &nrz)) return 0;
-  b.npairs = (d->nx - 4) / 2;
+  b.npairs = (b.p.xhi - b.p.xlo + 1) / 2;
   dim3 grid((unsigned)((long)b.nry * nrz), (unsigned)((b.npairs + TPB - 1) / TPB));
   if (d->parity == 0) lbib_fluid_step_x2<0><<<grid, TPB, 0, d->stream>>>(b);
   else lbib_fluid_step_x2<1><<<grid, TPB, 0, d->stream>>>(b);

@@ -3,8 +3,9 @@
  * translation units.  Not installed; include/lbib.h is the public ABI.
  *
  * GPU data layout (one fluid grid, several sheets):
- *   f        [19][N] populations (FP64; FP32; FP16 or BF16 holding f - w_q),
- *            N = nx*ny*nz, idx = (z*ny + y)*nx + x.
+ *   f        [19][Ns] populations (FP64; FP32; FP16 or BF16 holding f - w_q),
+ *            Ns = sx*ny*nz, idx = (z*ny + y)*sx + x - gx0: the whole grid
+ *            (sx = nx, gx0 = 0), or an x-slab of it with ghost columns.
  *            One buffer, updated in place with the AA access pattern; `parity`
  *            says how the next fused step must read it (0: each cell's own
  *            slots in natural order; 1: the neighbours' opposite slots).
@@ -51,7 +52,14 @@ typedef struct lbib_sheet_dev {
 
 typedef struct lbib_device {
   int nx, ny, nz;
-  long N;
+  long N;                        /* cells of the global grid                 */
+  /* the x-slab this state holds: global columns [x_lo, x_hi), stored with
+     two ghost columns on each side (the whole grid: [0, nx), no ghosts) */
+  int x_lo, x_hi;
+  int sx, gx0;                   /* stored row length; global x of column 0  */
+  long Ns;                       /* stored cells: sx * ny * nz               */
+  double* halo;                  /* slab exchange buffers [4][5][ny*nz]:     */
+                                 /* send_lo, send_hi, recv_lo, recv_hi       */
   int cube_size, ncx, ncy, ncz;
   int compat;
   int zin_hi;                    /* last z row the inlet/outlet copy reaches  */
@@ -119,11 +127,21 @@ typedef struct lbib_device {
 
 typedef struct lbdev_config {
   int nx, ny, nz, cube_size, compat, prec;
+  int x_lo, x_hi;                /* slab columns; x_hi = 0: the whole grid */
   double tau, u_l, rho_l, Ks_l, Kb_l, g_l, cs_l;
   int dt;
 } lbdev_config;
 
 int  lbdev_create(lbib_device** out, const lbdev_config* cfg);
+/* Columns [x_lo, x_hi) of the grid held by d (x_hi <= 0: all); sets the
+ * storage geometry, allocates nothing. */
+int  lbdev_set_columns(lbib_device* d, int x_lo, int x_hi);
+/* Slab exchange (FP64 slabs): after a fused step of parity `par`, pack the
+ * columns the neighbours need into send_lo / send_hi; after the transport,
+ * unpack recv_lo / recv_hi into this slab's columns. */
+int  lbdev_slab_pack(lbib_device* d, int par);
+int  lbdev_slab_unpack(lbib_device* d, int par);
+int  lbdev_slab_moments(lbib_device* d, double** U, long* n, int* failed_step);
 size_t lbdev_pop_bytes(int prec);
 /* The low-precision shift s_q and the (rho, u_x) it carries. */
 void lbdev_shift(const lbib_device* d, float* sh, double* rhos, double* uxs);

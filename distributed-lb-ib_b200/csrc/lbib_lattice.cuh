@@ -22,6 +22,12 @@
  *     num_cubes_x clip skips (yskip_z0, yskip_z0+1), for links from outside
  *     in y only -- from the second step on.
  *
+ * Storage: a state may hold only an x-slab of the lattice (columns
+ * [olo, ohi) of the global grid, plus two ghost columns on each side); all
+ * coordinates in the kernels are global, and a cell's slot index is
+ * ((z ny + y) sx + x - gx0) with sx the stored row length.  The whole
+ * lattice is the slab [0, nx) with sx = nx, gx0 = 0.
+ *
  * AA pattern (Bailey et al., 2009) in one buffer f[q][cell]:
  *   even step: read own slot q, write own slot opp(q);
  *   odd step:  read slot opp(q) of x - c_q, write slot q of x + c_q.
@@ -94,8 +100,11 @@ struct FluidParamsT {
   T* f;
   const R* inlet;
   const R* outlet;
-  long N;
-  int nx, ny, nz;
+  long N;                /* stored cells: the slot stride */
+  int nx, ny, nz;        /* the global grid */
+  int sx, gx0;           /* stored row length; global x of stored column 0 */
+  int olo, ohi;          /* columns this state owns: [olo, ohi) */
+  int xlo, xhi;          /* columns of I it collides: [xlo, xhi] */
   int zin_hi, yskip_z0, first;
   double rho0, ux0;
   double omtau, invtau, kw0, kw1, kw2, cs2, cs4, half_dt, g;
@@ -140,6 +149,12 @@ __device__ __forceinline__ int classify(const P& p, int x, int y, int z) {
   return K_FAST;
 }
 
+/* Slot index of global cell (x, y, z) in this state's storage. */
+template <typename P>
+__device__ __forceinline__ long sidx(const P& p, int x, int y, int z) {
+  return ((long)z * p.ny + y) * p.sx + (x - p.gx0);
+}
+
 __device__ __forceinline__ long link_offset(int q, long sy, long sz) {
   return (long)cx(q) + (long)cy(q) * sy + (long)cz(q) * sz;
 }
@@ -159,7 +174,7 @@ __device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y,
     for (int q = 0; q < 19; ++q) f[q] = t[q * P + pi];
     return;
   }
-  const long sy = p.nx, sz = (long)p.nx * p.ny;
+  const long sy = p.sx, sz = (long)p.sx * p.ny;
   if (kind == K_FAST) {
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
@@ -196,7 +211,7 @@ __device__ __forceinline__ void store_post(const FluidParamsT<T>& p, int x, int 
     for (int q = 0; q < 19; ++q) F[opp(q) * N + idx] = Pop<T>::put(f[q]);
     return;
   }
-  const long sy = p.nx, sz = (long)p.nx * p.ny;
+  const long sy = p.sx, sz = (long)p.sx * p.ny;
   if (kind == K_FAST) {
 #pragma unroll
     for (int q = 0; q < 19; ++q) F[q * N + idx + link_offset(q, sy, sz)] = Pop<T>::put(f[q]);

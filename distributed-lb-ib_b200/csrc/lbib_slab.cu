@@ -1,0 +1,134 @@
+/*
+ * x-slab decomposition of one grid over several states (one per GPU):
+ * the exchange of the columns next to a slab face.  No reference
+ * counterpart (the reference's pthread and MPI versions split the grid into
+ * cubes inside one address space or exchange whole cube faces with MPI).
+ *
+ * With the AA pattern only the odd step reaches across a face, and a slot
+ * of a column is read and written in the odd step by the same cell.  Slots
+ * of column X with c_x = -1 are read and written by cell X + 1, those with
+ * c_x = +1 by cell X - 1.  So, for a slab owning columns [lo, hi):
+ *   after an even step (fill):  the ghost column lo-1 needs the c_x = -1
+ *     slots of the left neighbour's column lo-1, and the ghost column hi
+ *     the c_x = +1 slots of the right neighbour's column hi;
+ *   after an odd step (flush):  what this slab's cells pushed into those
+ *     ghost slots goes back to the neighbours' columns lo-1 and hi.
+ * Only rows where both ends of the link lie in I cross: elsewhere the
+ * bounce-back keeps a link inside its cell.  Each message is 5 slots x ny
+ * x nz values.  The transport between slabs
+ * (a copy on one GPU, NCCL send/recv, or host staging) belongs to the
+ * caller: send_lo goes to the left neighbour's recv_hi, send_hi to the
+ * right neighbour's recv_lo.
+ */
+#include "lbib_internal.h"
+#include "lbib_lattice.cuh"
+
+using namespace lbib;
+
+namespace {
+
+/* The five directions with c_x = SIGN, in index order. */
+template <int SIGN>
+__device__ __forceinline__ int face_q(int j) {
+  return SIGN > 0 ? (j == 0 ? 1 : j == 1 ? 7 : j == 2 ? 9 : j == 3 ? 15 : 17)
+                  : (j == 0 ? 2 : j == 1 ? 8 : j == 2 ? 10 : j == 3 ? 16 : 18);
+}
+
+/* y or z offset of direction face_q(j). */
+template <int SIGN>
+__device__ __forceinline__ void face_cyz(int j, int& dy, int& dz) {
+  const int q = face_q<SIGN>(j);
+  dy = cy(q);
+  dz = cz(q);
+}
+
+/* buf[j][z ny + y] <-> f[face_q(j)][(z ny + y) sx + col].  Unpacking writes
+ * only the entries a step moves across the face: rows (y, z) of I whose
+ * source row (y - c_y, z - c_z) is in I too.  For the other rows the
+ * receiving slab's own cell has written the slot itself (a push whose
+ * target is outside I goes to the cell's own opposite slot), and the
+ * sender's ghost holds nothing. */
+template <int SIGN, bool PACK>
+__global__ void lbib_halo_copy(double* __restrict__ f, long Ns, int sx, int ny, int nz, int col,
+                               double* __restrict__ buf) {
+  const long P = (long)ny * nz;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  const int y = (int)(i % ny), z = (int)(i / ny);
+  const long idx = i * sx + col;
+  const bool row_in = y >= 2 && y <= ny - 3 && z >= 2 && z <= nz - 3;
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    double* a = f + face_q<SIGN>(j) * Ns + idx;
+    if (PACK) {
+      buf[j * P + i] = *a;
+    } else {
+      int dy, dz;
+      face_cyz<SIGN>(j, dy, dz);
+      const int ys = y - dy, zs = z - dz;
+      if (row_in && ys >= 2 && ys <= ny - 3 && zs >= 2 && zs <= nz - 3) *a = buf[j * P + i];
+    }
+  }
+}
+
+int halo_copy(lbib_device* d, int sign, bool pack, int x, double* buf) {
+  const long P = (long)d->ny * d->nz;
+  const int col = x - d->gx0;
+  double* f = (double*)d->f;
+  const unsigned nb = (unsigned)((P + 255) / 256);
+  if (sign > 0) {
+    if (pack) lbib_halo_copy<1, true><<<nb, 256, 0, d->stream>>>(f, d->Ns, d->sx, d->ny, d->nz, col, buf);
+    else lbib_halo_copy<1, false><<<nb, 256, 0, d->stream>>>(f, d->Ns, d->sx, d->ny, d->nz, col, buf);
+  } else {
+    if (pack) lbib_halo_copy<-1, true><<<nb, 256, 0, d->stream>>>(f, d->Ns, d->sx, d->ny, d->nz, col, buf);
+    else lbib_halo_copy<-1, false><<<nb, 256, 0, d->stream>>>(f, d->Ns, d->sx, d->ny, d->nz, col, buf);
+  }
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace
+
+/* Buffers: halo + k * 5P, k = 0 send_lo, 1 send_hi, 2 recv_lo, 3 recv_hi. */
+extern "C" int lbdev_slab_pack(lbib_device* d, int par) {
+  if (!d->halo) return -4;
+  const long P5 = 5L * d->ny * d->nz;
+  const int lo = d->x_lo > 0, hi = d->x_hi < d->nx;
+  if (par == 0) {        /* fill */
+    if (lo && halo_copy(d, +1, true, d->x_lo, d->halo)) return -2;
+    if (hi && halo_copy(d, -1, true, d->x_hi - 1, d->halo + P5)) return -2;
+  } else {               /* flush */
+    if (lo && halo_copy(d, -1, true, d->x_lo - 1, d->halo)) return -2;
+    if (hi && halo_copy(d, +1, true, d->x_hi, d->halo + P5)) return -2;
+  }
+  return 0;
+}
+
+extern "C" int lbdev_slab_unpack(lbib_device* d, int par) {
+  if (!d->halo) return -4;
+  const long P5 = 5L * d->ny * d->nz;
+  const int lo = d->x_lo > 0, hi = d->x_hi < d->nx;
+  if (par == 0) {        /* fill */
+    if (lo && halo_copy(d, -1, false, d->x_lo - 1, d->halo + 2 * P5)) return -2;
+    if (hi && halo_copy(d, +1, false, d->x_hi, d->halo + 3 * P5)) return -2;
+  } else {               /* flush */
+    if (lo && halo_copy(d, +1, false, d->x_lo, d->halo + 2 * P5)) return -2;
+    if (hi && halo_copy(d, -1, false, d->x_hi - 1, d->halo + 3 * P5)) return -2;
+  }
+  return 0;
+}
+
+/* This step's moment tiles (device) and their length in doubles, after the
+ * tile-moment kernel; waits for the stream.  Also reads the error word:
+ * returns its code (a stencil left the grid at step *failed_step). */
+extern "C" int lbdev_slab_moments(lbib_device* d, double** U, long* n, int* failed_step) {
+  int cnt = 0;
+  if (cudaMemcpyAsync(&cnt, d->tile_count[d->cur], sizeof(int), cudaMemcpyDeviceToHost, d->stream) != cudaSuccess)
+    return -2;
+  if (cudaMemcpyAsync(d->h_err, d->err, sizeof(int) * 2, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess) return -2;
+  if (cudaStreamSynchronize(d->stream) != cudaSuccess) return -2;
+  *U = d->Utile[d->cur];
+  *n = (long)cnt * 256;
+  if (failed_step) *failed_step = d->h_err[1];
+  return d->h_err[0];
+}

@@ -5,13 +5,14 @@
  * Compile with -fmad=false: the arithmetic is the generic kernel's
  * (collide/moments in lbib_lattice.cuh), bit for bit.
  *
- * Cells: y in [3, ny-4], z in [3, min(nz-4, zin_hi)], x in [2, nx-3]; every
- * link comes from a cell of I, so the only special cells are the plane cells
- * x = 2 and x = nx-3 (fixed inlet/outlet table).  Rows next to the walls run
+ * Cells: y in [3, ny-4], z in [3, min(nz-4, zin_hi)], x in [xlo, xhi] (the
+ * state's columns of I); every link comes from a cell of I, so the only
+ * special cells are the plane cells x = 2 and x = nx-3 (fixed inlet/outlet
+ * table).  Rows next to the walls run
  * the one-cell-per-thread generic kernel.
  *
- * A thread owns the pair (x, x+1), x even (nx is even, so I's x range
- * [2, nx-3] splits into pairs).  Even step: own slots, all 19 loads and
+ * A thread owns the pair (x, x+1), x even (nx and the slab bounds are
+ * even, so the x range splits into pairs).  Even step: own slots, all 19 loads and
  * stores are aligned double2.  Odd step: for the 9 directions with c_x = 0
  * the source and target pairs are aligned double2 too; for the 10 with
  * c_x = +-1 they are shifted by one cell, and the thread uses two 8-byte
@@ -64,8 +65,8 @@ __device__ __forceinline__ void x2_load_one(const FluidParams& p, int x, int y, 
 /* The step of the pair (x, x+1) of row (y, z); x even. */
 template <int PAR>
 __device__ __forceinline__ void x2_pair(const FluidParams& p, int x, int y, int z) {
-  const long idx = ((long)z * p.ny + y) * p.nx + x;
-  const long N = p.N, sy = p.nx, sz = (long)p.nx * p.ny;
+  const long idx = sidx(p, x, y, z);
+  const long N = p.N, sy = p.sx, sz = (long)p.sx * p.ny;
   const bool pa = (x == 2), pb = (x + 1 == p.nx - 3);
   double* __restrict__ F = p.f;
   double fa[19], fb[19];

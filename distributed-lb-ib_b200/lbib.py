@@ -59,6 +59,8 @@ EXPORTED = [
     "lbib_mlp_create", "lbib_mlp_free", "lbib_mlp_param_count", "lbib_mlp_stream", "lbib_mlp_get_params",
     "lbib_mlp_set_params", "lbib_mlp_forward", "lbib_mlp_gradient", "lbib_mlp_train_step", "lbib_mlp_synchronize",
     "lbib_save_restart", "lbib_load_restart", "lbib_mlp_set_stream",
+    "lbib_set_slab", "lbib_case_create_slab", "lbib_slab_buffers", "lbib_slab_step_fluid",
+    "lbib_slab_step_moments", "lbib_slab_moments", "lbib_slab_step_move",
 ]
 
 _dp = C.POINTER(C.c_double)

@@ -137,6 +137,7 @@ typedef struct gv_t {
   int lbib_compat;                 /* LBIB_COMPAT_* bits, see below      */
   int lbib_dump_mode;              /* LBIB_DUMP_* bits for do_thread     */
   int lbib_precision;              /* LBIB_PREC_* population storage     */
+  int lbib_slab_lo, lbib_slab_hi;  /* x-slab held here; hi = 0: all      */
 }* GV;
 
 /* mpi/do_thread.h:242-245 */
@@ -288,6 +289,45 @@ int lbib_sync_to_host(GV gv);
 /* Frees everything this library allocated for gv (GPU state, sheets,
  * fluid_grid planes); gv itself and the objects the caller made stay. */
 void lbib_free(GV gv);
+
+/* x-slab decomposition over several GPUs (no counterpart in the reference:
+ * its pthread version shares one address space, its MPI version exchanges
+ * whole cube faces).  Each GV holds the global columns [x_lo, x_hi) of the
+ * grid (multiples of 4; FP64 storage) plus two ghost columns on each side,
+ * and the whole sheet, whose forces, spread and move every slab computes
+ * alike.  A step is three calls with two exchanges between them:
+ *   par = lbib_slab_step_fluid(gv)  forces, spread, fused fluid step on this
+ *                                   slab's cells; packs the face columns
+ *                                   into send_lo / send_hi; returns the
+ *                                   step's AA parity (0 or 1) or an error;
+ *   exchange 1: send_lo -> left neighbour's recv_hi, send_hi -> right
+ *               neighbour's recv_lo (5*ny*nz doubles each);
+ *   lbib_slab_step_moments(gv)      unpacks recv_lo / recv_hi and computes
+ *                                   the moment tiles of this slab's columns
+ *                                   (-0.0 in the others);
+ *   lbib_slab_moments(gv, &U, &n)   the moment tiles (n doubles on the
+ *                                   device; waits for the stream) and the
+ *                                   step's error code;
+ *   exchange 2: U <- sum of U over all slabs (each value is owned by one
+ *               slab and -0.0 elsewhere, so the sum keeps every bit);
+ *   lbib_slab_step_move(gv)         moves the sheet; advances gv->time.
+ * All device work goes on lbib_stream(gv); the exchanges must be ordered
+ * after and before it.  With the slabs' results put together the run is
+ * bit-identical to the whole grid on one GPU.  lbib_run refuses a slab
+ * (LBIB_E_STATE), as do the restart files. */
+int lbib_set_slab(GV gv, int x_lo, int x_hi);   /* like lbib_set_precision: before init_gv */
+GV lbib_case_create_slab(int nx, int ny, int nz, int cube_size, int nsheets,
+                         const int* rows, const int* cols,
+                         const double* width, const double* height,
+                         const double* x0, const double* y0, const double* z0,
+                         double tau, double u_l, double Ks_l, double Kb_l, int compat,
+                         int x_lo, int x_hi);
+/* bufs[4] = device pointers send_lo, send_hi, recv_lo, recv_hi; *len = doubles each */
+int lbib_slab_buffers(GV gv, double** bufs, long* len);
+int lbib_slab_step_fluid(GV gv);
+int lbib_slab_step_moments(GV gv);
+int lbib_slab_moments(GV gv, double** U, long* n);
+int lbib_slab_step_move(GV gv);
 
 /* Restart files (no counterpart in the reference, which can only restart
  * from its initial state): lbib_save_restart writes everything the next

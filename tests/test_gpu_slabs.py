@@ -1,0 +1,87 @@
+"""The x-slab decomposition on the GPU: slabs advanced together (in one
+process, and as two gloo ranks exchanging through host memory) give the
+whole grid's run bit for bit -- sheet, populations and moments -- with the
+sheet's stencil crossing a slab face."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import lbib
+import slabs
+from cases import c0_case, small_case
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize("bounds", [[(0, 20), (20, 68), (68, 128)], [(0, 64), (64, 128)]])
+def test_local_slabs_equal_whole_grid(gpu, bounds):
+    case, steps = c0_case(), 25
+    with lbib.Solver(case) as whole:
+        whole.run(steps)
+        sheet, df1, mom = whole.sheet(), whole.df1(), whole.moments()
+    with slabs.LocalSlabs(case, bounds=bounds) as L:
+        L.run(steps)
+        assert np.array_equal(L.sheet(), sheet)
+        assert np.array_equal(L.df1()[:, 2:-2, 2:-2, 2:-2], df1[:, 2:-2, 2:-2, 2:-2])
+        for a, b in zip(L.moments(), mom):
+            assert np.array_equal(a, b)
+        # the sheet moved, and the run reached odd and even parities
+        assert np.abs(sheet[..., 0] - L.slabs[0].case.sheets[0].x0).max() > 0
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _slab_case():
+    return small_case(64, 16, 16, 8, 8, x0=30.0)
+
+
+def _rank_main(rank, world, port, steps, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    for p in (os.path.join(ROOT, "distributed-lb-ib_b200"), os.path.join(ROOT, "tests"),
+              os.path.join(ROOT, "oracle")):
+        sys.path.insert(0, p)
+    import datetime
+    import torch.distributed as dist
+    import slabs as S
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    d = S.DistSlabs(case=_slab_case())
+    d.run(steps)
+    s = d.slab
+    q.put((rank, s.x_lo, s.x_hi, s.sheet(), s.df1()[:, :, :, s.columns]))
+    dist.barrier()
+    d.close()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_gloo_equal_whole_grid(gpu):
+    steps, world = 31, 2
+    case = _slab_case()
+    with lbib.Solver(case) as whole:
+        whole.run(steps)
+        sheet, df1 = whole.sheet(), whole.df1()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, steps, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    got = np.zeros_like(df1)
+    for rank, lo, hi, sh, part in out:
+        assert np.array_equal(sh, sheet), rank
+        got[:, :, :, lo:hi] = part
+    assert np.array_equal(got[:, 2:-2, 2:-2, 2:-2], df1[:, 2:-2, 2:-2, 2:-2])
