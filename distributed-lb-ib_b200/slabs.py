@@ -312,3 +312,92 @@ class _Null:
 
     def __exit__(self, *a):
         return False
+
+
+def _case(a):
+    from types import SimpleNamespace as NS
+    w, h = 0.5 * (a.cols - 1), 0.5 * (a.rows - 1)
+    sheet = NS(rows=a.rows, cols=a.cols, width=w, height=h, x0=a.x0,
+               y0=(a.ny - 1) / 2.0 - h / 2.0, z0=(a.nz - 1) / 2.0 - w / 2.0)
+    return NS(nx=a.nx, ny=a.ny, nz=a.nz, cube_size=4, tau=0.6, u_l=0.01, Ks_l=0.05, Kb_l=0.005,
+              compat=lbib.COMPAT_ALL, sheets=[sheet])
+
+
+def main(argv=None) -> int:
+    """Time the slab decomposition.  Under torch.distributed.run (one rank per
+    GPU, NCCL): one slab per rank, CUDA-event time on each slab's stream, max
+    over ranks.  With --local N: N slabs in this process on one GPU (the
+    host-synchronised transport, wall-clock per step), compared bit for bit
+    with the whole grid run alongside."""
+    import argparse
+    import json
+    import os
+    import time
+
+    import torch
+
+    ap = argparse.ArgumentParser(description="x-slab decomposition timing")
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--ny", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=256)
+    ap.add_argument("--rows", type=int, default=208)
+    ap.add_argument("--cols", type=int, default=208)
+    ap.add_argument("--x0", type=float, default=80.0)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--local", type=int, default=0, help="N slabs in one process on one GPU")
+    a = ap.parse_args(argv)
+    case = _case(a)
+    cells = a.nx * a.ny * a.nz
+    out = {"lattice": [a.nx, a.ny, a.nz], "sheet": [a.rows, a.cols], "steps": a.steps, "warmup": a.warmup}
+    if a.local:
+        L = LocalSlabs(case, n=a.local)
+        L.run(a.warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.run(a.steps)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / a.steps
+        with lbib.Solver(case) as W:
+            W.run(a.warmup)
+            W.synchronize()
+            t0 = time.perf_counter()
+            W.run(a.steps)
+            W.synchronize()
+            wms = (time.perf_counter() - t0) * 1e3 / a.steps
+            same = bool(np.array_equal(W.sheet(), L.sheet()))
+        L.close()
+        out.update(mode="local", slabs=a.local, bounds=L.bounds, ms_per_step=ms, mlups=cells / ms / 1e3,
+                   whole_ms_per_step=wms, whole_mlups=cells / wms / 1e3, sheet_bit_identical=same)
+        print(json.dumps(out))
+        return 0 if same else 1
+    import datetime
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    D = DistSlabs(case)
+    D.run(a.warmup)
+    s = torch.cuda.ExternalStream(D.slab.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(s)
+    D.run(a.steps)
+    e1.record(s)
+    e1.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1) / a.steps], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    if D.rank == 0:
+        out.update(mode="nccl", slabs=D.world, bounds=slab_bounds(a.nx, D.world), ms_per_step=ms,
+                   mlups=cells / ms / 1e3)
+        print(json.dumps(out))
+    D.close()
+    dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
