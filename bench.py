@@ -431,11 +431,16 @@ def run_sweep_leg(args, group):
     t16, t64 = np.array(out["f16-flow"].pop("tips")), np.array(out["f64"].pop("tips"))
     both = np.array(out["f16-flow"].pop("completed")) & np.array(out["f64"].pop("completed"))
     stopped16 = out["f16-flow"]["stopped"]
-    ok = both & (np.abs(t16 - t64) <= 0.02 * np.maximum(np.abs(t64), 1e-3))
+    rel = np.abs(t16 - t64) / np.maximum(np.abs(t64), 1e-3)
+    ok = both & (rel <= 0.02)
+    miss = [{"problem": int(i), "tip_fp64": float(t64[i]), "tip_fp16": float(t16[i])}
+            for i in np.nonzero(both & ~ok)[0]]
     return {"workload": f"{len(probs)} problems (sweep.py, seed 1), {args.sweep_steps} steps, one batch per GPU",
             "unit": "points/s", "fp16_batched": out["f16-flow"], "fp64_batched": out["f64"],
             "speedup_fp16_vs_fp64": out["f16-flow"]["points_per_s"] / out["f64"]["points_per_s"],
             "completed_both": int(both.sum()), "tip_within_2pct_of_fp64": int(ok.sum()), "stopped_fp16": stopped16,
+            "tip_rel_err_median": float(np.median(rel[both])) if both.any() else None,
+            "tip_outside_2pct": miss,
             "note": "a point whose sheet left its grid stops there and counts as run; tips are compared on "
                     "the points both runs completed"}
 
