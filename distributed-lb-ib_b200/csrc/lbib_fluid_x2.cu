@@ -13,8 +13,13 @@ namespace {
 
 constexpr int TPB = 128;
 
-#ifndef LBIB_X2_MINB
-#define LBIB_X2_MINB 3
+/* Resident blocks per SM each parity's kernel is compiled for (the register
+ * budget): 3 x 128 threads at up to 168 registers. */
+#ifndef LBIB_X2_MINB0
+#define LBIB_X2_MINB0 3
+#endif
+#ifndef LBIB_X2_MINB1
+#define LBIB_X2_MINB1 3
 #endif
 
 struct X2Params {
@@ -24,7 +29,7 @@ struct X2Params {
 };
 
 template <int PAR>
-__global__ void __launch_bounds__(TPB, LBIB_X2_MINB) lbib_fluid_step_x2(X2Params b) {
+__global__ void __launch_bounds__(TPB, PAR ? LBIB_X2_MINB1 : LBIB_X2_MINB0) lbib_fluid_step_x2(X2Params b) {
   const int pr = blockIdx.y * TPB + threadIdx.x;
   if (pr >= b.npairs) return;
   const int y = 3 + (int)(blockIdx.x % b.nry);
