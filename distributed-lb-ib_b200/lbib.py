@@ -261,9 +261,16 @@ class Solver:
         _check(self.lib.lbib_profile_end(self.gv, _ptr(ms), C.byref(n)), "lbib_profile_end")
         return dict(zip(["forces", "spread", "fluid", "moments", "move"], ms.tolist())), n.value
 
-    def moments(self):
+    def moments(self, out=None):
+        """rho, ux, uy, uz as (nz, ny, nx) arrays; `out` (four C-contiguous
+        float64 arrays of N values) is filled in place when given."""
         c = self.case
-        a = [np.empty(self.N) for _ in range(4)]
+        if out is None:
+            a = [np.empty(self.N) for _ in range(4)]
+        else:
+            a = list(out)
+            if len(a) != 4 or any(x.dtype != np.float64 or x.size != self.N or not x.flags.c_contiguous for x in a):
+                raise LbibError("moments(out=...): four C-contiguous float64 arrays of nx*ny*nz values")
         _check(self.lib.lbib_get_moments(self.gv, *[_ptr(x) for x in a]), "lbib_get_moments")
         return [x.reshape(c.nz, c.ny, c.nx) for x in a]
 

@@ -13,6 +13,7 @@ import torch.multiprocessing as mp
 import lbib
 import slabs
 from cases import c0_case, small_case
+from pyoracle import Case, Sheet
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -32,6 +33,17 @@ def test_local_slabs_equal_whole_grid(gpu, bounds):
             assert np.array_equal(a, b)
         # the sheet moved, and the run reached odd and even parities
         assert np.abs(sheet[..., 0] - L.slabs[0].case.sheets[0].x0).max() > 0
+
+
+def test_a_stencil_leaving_the_grid_stops_the_slabs(gpu):
+    # a sheet one cell from the outlet: its stencil leaves the grid within a few steps
+    bad = Case(32, 16, 16, [Sheet(4, 4, 1.5, 1.5, 29.3, 7.0, 7.0)], u_l=0.1)
+    with lbib.Solver(bad) as whole:
+        with pytest.raises(lbib.LbibError, match="stencil"):
+            whole.run(20)
+    with slabs.LocalSlabs(bad, bounds=[(0, 16), (16, 32)]) as L:
+        with pytest.raises(lbib.LbibError, match="stencil"):
+            L.run(20)
 
 
 def _free_port():
