@@ -124,10 +124,22 @@ void gen_fiber_sheet(Fibersheet* sheet) {
   int num_rows = sheet->num_rows;
   double zdist = width / (num_cols - 1);
   double ydist = height / (num_rows - 1);
+  /* The rows' node arrays are consecutive pieces of one page-aligned block
+     (the reference callocs each row): the block is the [rows*cols] record
+     layout of the GPU copy, so that, once page-locked at upload, the sheet
+     comes back from the GPU in one copy with no host-side repacking. */
+  const size_t page = 4096;
+  const size_t bytes = (size_t)num_rows * num_cols * sizeof(Fibernode);
+  Fibernode* block = NULL;
+  if (posix_memalign((void**)&block, page, (bytes + page - 1) / page * page) != 0) {
+    set_error(LBIB_E_NOMEM);
+    return;
+  }
+  memset(block, 0, (bytes + page - 1) / page * page);
   sheet->fibers = (Fiber*)calloc(num_rows, sizeof(Fiber));
   for (int row = 0; row < num_rows; ++row) {
     Fiber* fiber = sheet->fibers + row;
-    fiber->nodes = (Fibernode*)calloc(num_cols, sizeof(Fibernode));
+    fiber->nodes = block + (size_t)row * num_cols;
     fiber->num_nodes = num_cols;
     for (int col = 0; col < num_cols; ++col) {
       fiber->nodes[col].x = sheet->x_orig;
@@ -135,6 +147,15 @@ void gen_fiber_sheet(Fibersheet* sheet) {
       fiber->nodes[col].z = zdist * col + sheet->z_orig;
     }
   }
+}
+
+/* The sheet's rows lie back to back in one block (as gen_fiber_sheet makes
+ * them): its first node, else NULL. */
+static Fibernode* sheet_block(const Fibersheet* sh) {
+  if (!sh->fibers) return NULL;
+  for (int r = 1; r < sh->num_rows; ++r)
+    if (sh->fibers[r].nodes != sh->fibers[0].nodes + (size_t)r * sh->num_cols) return NULL;
+  return sh->fibers[0].nodes;
 }
 
 static long total_nodes(GV gv) {
@@ -186,6 +207,12 @@ static int upload_sheets(GV gv) {
   int rc = buf ? lbdev_set_sheets(gv->dev, shape->num_sheets, sh, buf) : LBIB_E_NOMEM;
   free(buf);
   free(sh);
+  /* page-lock the sheets' blocks for direct copies (best effort) */
+  for (int k = 0; !rc && k < shape->num_sheets; ++k) {
+    Fibersheet* s = &shape->sheets[k];
+    Fibernode* b = sheet_block(s);
+    if (b) lbdev_register_host(gv->dev, b, sizeof(Fibernode) * (size_t)s->num_rows * s->num_cols);
+  }
   return rc ? set_error(rc) : LBIB_OK;
 }
 
@@ -572,8 +599,27 @@ int lbib_sync_to_host(GV gv) {
   if (!gv || !gv->dev || !gv->fiber_shape) return set_error(LBIB_E_STATE);
   long S = total_nodes(gv);
   if (S != gv->dev->S) return set_error(LBIB_E_STATE);
-  int rc = lbdev_get_nodes(gv->dev, NULL);  /* into the pinned staging buffer */
-  if (!rc) unpack_nodes(gv, gv->dev->h_nodes);
+  /* every sheet's block page-locked: one direct copy each */
+  int direct = 1;
+  for (int k = 0; direct && k < gv->fiber_shape->num_sheets; ++k) {
+    const Fibersheet* sh = &gv->fiber_shape->sheets[k];
+    const Fibernode* b = sheet_block(sh);
+    direct = b && lbdev_is_registered(gv->dev, b, sizeof(Fibernode) * (size_t)sh->num_rows * sh->num_cols);
+  }
+  int rc = 0;
+  if (direct) {
+    long o = 0;
+    for (int k = 0; !rc && k < gv->fiber_shape->num_sheets; ++k) {
+      Fibersheet* sh = &gv->fiber_shape->sheets[k];
+      const long n = (long)sh->num_rows * sh->num_cols;
+      rc = lbdev_copy_nodes_out(gv->dev, o, n, (double*)sh->fibers[0].nodes);
+      o += n;
+    }
+    if (!rc) rc = lbdev_sync(gv->dev);
+  } else {
+    rc = lbdev_get_nodes(gv->dev, NULL);    /* into the pinned staging buffer */
+    if (!rc) unpack_nodes(gv, gv->dev->h_nodes);
+  }
   return rc ? set_error(rc) : LBIB_OK;
 }
 
@@ -736,7 +782,7 @@ void lbib_free(GV gv) {
     for (int k = 0; k < gv->fiber_shape->num_sheets; ++k) {
       Fibersheet* sh = &gv->fiber_shape->sheets[k];
       if (!sh->fibers) continue;
-      for (int r = 0; r < sh->num_rows; ++r) free(sh->fibers[r].nodes);
+      free(sh->fibers[0].nodes);      /* the block of all rows (gen_fiber_sheet) */
       free(sh->fibers);
       sh->fibers = NULL;
     }

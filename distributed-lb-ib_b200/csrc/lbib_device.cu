@@ -266,6 +266,7 @@ extern "C" void lbdev_free(lbib_device* d) {
   cudaFree(d->f); cudaFree(d->inlet); cudaFree(d->outlet); cudaFree(d->err); cudaFree(d->rows);
   cudaFree(d->halo);
   cudaFree(d->scratch);
+  for (int i = 0; i < d->nhost_reg; ++i) cudaHostUnregister(d->host_reg[i]);
   for (long i = 0; i < 6 * d->prof_cap; ++i) cudaEventDestroy(d->prof_ev[i]);
   free(d->prof_ev);
   if (d->h_err) cudaFreeHost(d->h_err);
@@ -525,6 +526,30 @@ extern "C" int lbdev_get_nodes(lbib_device* d, double* out) {
   CK(cudaMemcpyAsync(d->h_nodes, d->nodes, sizeof(double) * 12 * d->S, cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));
   if (out) memcpy(out, d->h_nodes, sizeof(double) * 12 * d->S);
+  return 0;
+}
+
+extern "C" int lbdev_register_host(lbib_device* d, void* p, size_t bytes) {
+  if (d->nhost_reg >= 8 || lbdev_is_registered(d, p, bytes)) return 0;
+  if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) != cudaSuccess) {
+    cudaGetLastError();                /* not fatal: copies go through staging */
+    return -2;
+  }
+  d->host_reg[d->nhost_reg] = p;
+  d->host_reg_bytes[d->nhost_reg] = bytes;
+  d->nhost_reg++;
+  return 0;
+}
+
+extern "C" int lbdev_is_registered(const lbib_device* d, const void* p, size_t bytes) {
+  for (int i = 0; i < d->nhost_reg; ++i)
+    if (d->host_reg[i] == p && d->host_reg_bytes[i] == bytes) return 1;
+  return 0;
+}
+
+extern "C" int lbdev_copy_nodes_out(lbib_device* d, long first, long n, double* host) {
+  if (first < 0 || n < 0 || first + n > d->S) return -1;
+  CK(cudaMemcpyAsync(host, d->nodes + 12 * first, sizeof(double) * 12 * n, cudaMemcpyDeviceToHost, d->stream));
   return 0;
 }
 

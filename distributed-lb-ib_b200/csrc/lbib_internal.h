@@ -114,6 +114,9 @@ typedef struct lbib_device {
   int* err;                      /* [2]: code, step                           */
   int* h_err;                    /* pinned mirror                             */
   double* scratch;               /* dense field scratch for getters           */
+  void* host_reg[8];             /* host blocks page-locked for direct copies */
+  size_t host_reg_bytes[8];
+  int nhost_reg;
   cudaStream_t stream;
   int device;
   long kernel_launches;          /* kernels this state has launched           */
@@ -161,6 +164,12 @@ int  lbdev_conservation(lbib_device* d, double* out);
 int  lbdev_get_nodes(lbib_device* d, double* out);
 int  lbdev_set_nodes(lbib_device* d, const double* in);
 int  lbdev_sync(lbib_device* d);
+/* Page-lock a host block the library owns (a sheet's node records) so that
+ * copies go to it directly; best effort, undone by lbdev_free. */
+int  lbdev_register_host(lbib_device* d, void* p, size_t bytes);
+int  lbdev_is_registered(const lbib_device* d, const void* p, size_t bytes);
+/* Node records [first, first+n) to host memory, asynchronous on the stream. */
+int  lbdev_copy_nodes_out(lbib_device* d, long first, long n, double* host);
 int  lbdev_variants(const lbib_device* d);     /* kernel variants for this precision */
 int  lbdev_set_variant(lbib_device* d, int v);
 /* Times every variant on fluid steps from the initial state, keeps the
