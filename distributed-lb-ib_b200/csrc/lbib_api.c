@@ -661,31 +661,18 @@ static long sheet_offset(GV gv, int sheet) {
 int lbib_get_sheet(GV gv, int sheet, double* out) {
   if (!gv || !gv->dev || !gv->fiber_shape) return set_error(LBIB_E_STATE);
   if (!out || sheet < 0 || sheet >= gv->fiber_shape->num_sheets) return set_error(LBIB_E_ARG);
-  long S = gv->dev->S;
-  double* buf = (double*)malloc(sizeof(double) * 12 * S);
-  if (!buf) return set_error(LBIB_E_NOMEM);
-  int rc = lbdev_get_nodes(gv->dev, buf);
-  if (!rc) {
-    Fibersheet* sh = &gv->fiber_shape->sheets[sheet];
-    memcpy(out, buf + sheet_offset(gv, sheet) * 12, sizeof(double) * 12 * sh->num_rows * sh->num_cols);
-  }
-  free(buf);
+  const Fibersheet* sh = &gv->fiber_shape->sheets[sheet];
+  int rc = lbdev_copy_nodes_out(gv->dev, sheet_offset(gv, sheet), (long)sh->num_rows * sh->num_cols, out);
+  if (!rc) rc = lbdev_sync(gv->dev);
   return rc ? set_error(rc) : LBIB_OK;
 }
 
 int lbib_set_sheet(GV gv, int sheet, const double* in) {
   if (!gv || !gv->dev || !gv->fiber_shape) return set_error(LBIB_E_STATE);
   if (!in || sheet < 0 || sheet >= gv->fiber_shape->num_sheets) return set_error(LBIB_E_ARG);
-  long S = gv->dev->S;
-  double* buf = (double*)malloc(sizeof(double) * 12 * S);
-  if (!buf) return set_error(LBIB_E_NOMEM);
-  int rc = lbdev_get_nodes(gv->dev, buf);
-  if (!rc) {
-    Fibersheet* sh = &gv->fiber_shape->sheets[sheet];
-    memcpy(buf + sheet_offset(gv, sheet) * 12, in, sizeof(double) * 12 * sh->num_rows * sh->num_cols);
-    rc = lbdev_set_nodes(gv->dev, buf);
-  }
-  free(buf);
+  const Fibersheet* sh = &gv->fiber_shape->sheets[sheet];
+  int rc = lbdev_copy_nodes_in(gv->dev, sheet_offset(gv, sheet), (long)sh->num_rows * sh->num_cols, in);
+  if (!rc) rc = lbdev_sync(gv->dev);
   return rc ? set_error(rc) : LBIB_OK;
 }
 

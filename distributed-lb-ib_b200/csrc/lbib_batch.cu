@@ -288,7 +288,7 @@ int build_word_blocks(lbib_batch* b) {
       int nry = 0, nrz = 0;
       if (b->variant[k] != v || !b->h_desc[k].bulk || !lbdev_bulk_rows(b->sh[k], &nry, &nrz)) continue;
       const int V = batch_variant_cells_lp(b->prec, v);
-      const long gpr = (b->sh[k]->nx / V + 31) / 32 * 32;
+      const long gpr = b->sh[k]->nx / V;   /* words_geometry: rows end to end */
       n += ((long)nry * nrz * gpr + WTPB - 1) / WTPB;
     }
     if (!n) continue;
@@ -299,7 +299,7 @@ int build_word_blocks(lbib_batch* b) {
       int nry = 0, nrz = 0;
       if (b->variant[k] != v || !b->h_desc[k].bulk || !lbdev_bulk_rows(b->sh[k], &nry, &nrz)) continue;
       const int V = batch_variant_cells_lp(b->prec, v);
-      const long gpr = (b->sh[k]->nx / V + 31) / 32 * 32;
+      const long gpr = b->sh[k]->nx / V;   /* words_geometry: rows end to end */
       const long nb = ((long)nry * nrz * gpr + WTPB - 1) / WTPB;
       for (long j = 0; j < nb; ++j) h[i++] = make_int2(k, (int)j);
     }

@@ -553,6 +553,12 @@ extern "C" int lbdev_copy_nodes_out(lbib_device* d, long first, long n, double* 
   return 0;
 }
 
+extern "C" int lbdev_copy_nodes_in(lbib_device* d, long first, long n, const double* host) {
+  if (first < 0 || n < 0 || first + n > d->S) return -1;
+  CK(cudaMemcpyAsync(d->nodes + 12 * first, host, sizeof(double) * 12 * n, cudaMemcpyHostToDevice, d->stream));
+  return 0;
+}
+
 extern "C" int lbdev_set_nodes(lbib_device* d, const double* in) {
   CK(cudaMemcpyAsync(d->nodes, in, sizeof(double) * 12 * d->S, cudaMemcpyHostToDevice, d->stream));
   CK(cudaStreamSynchronize(d->stream));

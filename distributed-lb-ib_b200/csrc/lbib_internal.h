@@ -170,6 +170,7 @@ int  lbdev_register_host(lbib_device* d, void* p, size_t bytes);
 int  lbdev_is_registered(const lbib_device* d, const void* p, size_t bytes);
 /* Node records [first, first+n) to host memory, asynchronous on the stream. */
 int  lbdev_copy_nodes_out(lbib_device* d, long first, long n, double* host);
+int  lbdev_copy_nodes_in(lbib_device* d, long first, long n, const double* host);
 int  lbdev_variants(const lbib_device* d);     /* kernel variants for this precision */
 int  lbdev_set_variant(lbib_device* d, int v);
 /* Times every variant on fluid steps from the initial state, keeps the

@@ -8,7 +8,11 @@
  * aligned too.  Odd step, c_x = +-1: the V values a thread needs are its own
  * word shifted by one element, the missing element coming from the
  * neighbouring lane's word (one 32-bit shuffle and a byte_perm); pushes are
- * assembled the same way before the store.  At a warp edge (lane 0 / 31) the
+ * assembled the same way before the store.  Rows are packed end to end in
+ * the thread space (a warp may hold the end of one row and the start of the
+ * next): the groups that collide here never are a row's first or last word,
+ * so their neighbouring words are always the next lanes' of the same row,
+ * or lie across a warp edge.  At a warp edge (lane 0 / 31) the
  * element crosses to another warp, and the thread that owns the pushing cell
  * reads and writes it with a scalar access -- the AA rule that a slot is
  * read and written only by the cell that pushes into it keeps that
@@ -124,7 +128,7 @@ struct WordsParams {
   int nry;      /* bulk rows in y */
   long nrows;   /* bulk rows */
   int ngroups;  /* words per x row: nx / V */
-  int gpr;      /* threads per row: ngroups rounded up to whole warps */
+  int gpr;      /* threads per row: ngroups (rows packed end to end) */
   int g0, g1;   /* groups whose cells all lie in [4, nx-5] */
 };
 
@@ -434,7 +438,7 @@ __host__ __forceinline__ void words_geometry(WordsParams<T>& b, int V, int nx, i
   b.nry = nry;
   b.nrows = (long)nry * nrz;
   b.ngroups = nx / V;
-  b.gpr = (b.ngroups + 31) / 32 * 32;
+  b.gpr = b.ngroups;
   b.g0 = (4 + V - 1) / V;
   b.g1 = (nx - 4) / V - 1;
 }
