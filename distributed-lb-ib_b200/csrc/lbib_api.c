@@ -371,6 +371,75 @@ int lbib_slab_step_move(GV gv) {
   return LBIB_OK;
 }
 
+int lbib_slab_storage(GV gv, double** f, long* Ns, int* sx, int* gx0, double** U0, double** U1) {
+  if (!gv || !f || !Ns || !sx || !gx0 || !U0 || !U1) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv) || !gv->dev->Utile[0]) return set_error(LBIB_E_STATE);
+  lbib_device* d = gv->dev;
+  *f = (double*)d->f; *Ns = d->Ns; *sx = d->sx; *gx0 = d->gx0;
+  *U0 = d->Utile[0]; *U1 = d->Utile[1];
+  return LBIB_OK;
+}
+
+int lbib_slab_connect(GV gv, double* lo_f, long lo_Ns, int lo_sx, int lo_gx0, double* hi_f, long hi_Ns, int hi_sx,
+                      int hi_gx0, int n, double* const* U0, double* const* U1) {
+  if (!gv) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv)) return set_error(LBIB_E_STATE);
+  return lbdev_slab_connect(gv->dev, lo_f, lo_Ns, lo_sx, lo_gx0, hi_f, hi_Ns, hi_sx, hi_gx0, n, U0, U1)
+             ? set_error(LBIB_E_ARG) : LBIB_OK;
+}
+
+int lbib_slab_step_fluid_direct(GV gv) {
+  if (!gv) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv) || gv->dev->npeer_U < 1) return set_error(LBIB_E_STATE);
+  lbib_device* d = gv->dev;
+  static const int order[] = {0, 3, 4};
+  for (int i = 0; i < 3; ++i) {
+    int rc = lbdev_stage(d, order[i], gv->time);
+    if (rc) return set_error(rc);
+  }
+  const int par = d->parity ^ 1;
+  int rc = lbdev_slab_push(d, par);
+  return rc ? set_error(rc == -4 ? LBIB_E_STATE : LBIB_E_CUDA) : par;
+}
+
+int lbib_slab_step_moments_direct(GV gv) {
+  if (!gv) return set_error(LBIB_E_ARG);
+  if (!is_slab(gv) || gv->dev->steps == 0 || gv->dev->npeer_U < 1) return set_error(LBIB_E_STATE);
+  int rc = lbdev_slab_moments_bcast(gv->dev);
+  return rc ? set_error(rc == -4 ? LBIB_E_STATE : LBIB_E_CUDA) : LBIB_OK;
+}
+
+int lbib_slab_check(GV gv) {
+  if (!gv || !gv->dev) return set_error(LBIB_E_STATE);
+  int failed = 0;
+  int e = lbdev_check(gv->dev, &failed);
+  if (e) {
+    if (e != LBIB_E_CUDA) gv->time = failed;
+    return set_error(e);
+  }
+  return LBIB_OK;
+}
+
+int lbib_peer_access(int device, int peer) {
+  int rc = lbdev_peer_access(device, peer);
+  return rc ? set_error(rc == -1 ? LBIB_E_ARG : LBIB_E_CUDA) : LBIB_OK;
+}
+
+int lbib_ipc_handle(void* dev_ptr, void* handle) {
+  if (!dev_ptr || !handle) return set_error(LBIB_E_ARG);
+  return lbdev_ipc_handle(dev_ptr, handle) ? set_error(LBIB_E_CUDA) : LBIB_OK;
+}
+
+int lbib_ipc_open(const void* handle, void** dev_ptr) {
+  if (!handle || !dev_ptr) return set_error(LBIB_E_ARG);
+  return lbdev_ipc_open(handle, dev_ptr) ? set_error(LBIB_E_CUDA) : LBIB_OK;
+}
+
+int lbib_ipc_close(void* dev_ptr) {
+  if (!dev_ptr) return set_error(LBIB_E_ARG);
+  return lbdev_ipc_close(dev_ptr) ? set_error(LBIB_E_CUDA) : LBIB_OK;
+}
+
 int lbib_kernel_variants(GV gv) {
   if (!gv || !gv->dev) return set_error(LBIB_E_STATE);
   return lbdev_variants(gv->dev);

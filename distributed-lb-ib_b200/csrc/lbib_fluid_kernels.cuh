@@ -233,33 +233,42 @@ __global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
   step_cell<T, PAR>(p, x, r.x, r.y);
 }
 
-/* (rho, u)(t) of every cell of the touched tiles, after the fused step of
- * parity 1-PAR: compute_rho_and_u (lbm_ib.c:2440-2538) restricted to where
- * moveFiberSheet will read.  Cells outside M keep the initial values.  A
- * tile outside this state's columns gets -0.0, the identity of a sum, so
- * that adding the tiles of all slabs gives every value with its bits. */
+/* (rho, u)(t) of cell `cell` of touched tile `tile` (slot i), after the
+ * fused step of parity 1-PAR: compute_rho_and_u (lbm_ib.c:2440-2538)
+ * restricted to where moveFiberSheet will read.  Cells outside M keep the
+ * initial values.  Returns false for a tile outside this state's columns
+ * (another slab owns it; the values are not computed). */
+template <typename T, int PAR>
+__device__ __forceinline__ bool tile_moment_values(const FluidParamsT<T>& p, int tile, int i, int cell,
+                                                   const double* __restrict__ Ftile, double& rho, double& ux,
+                                                   double& uy, double& uz) {
+  using R = typename Pop<T>::R;
+  const int tx = tile % p.ntx, ty = (tile / p.ntx) % p.nty, tz = tile / (p.ntx * p.nty);
+  if (tx * 4 < p.olo || tx * 4 >= p.ohi) return false;
+  const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
+  rho = p.rho0; ux = p.ux0; uy = 0.0; uz = 0.0;
+  if (x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
+    const long idx = sidx(p, x, y, z);
+    R f[19];
+    load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
+    const double* Ft = Ftile + (long)i * 192;
+    Mom<R> m;
+    Form<T>::moments(f, (R)Ft[cell], (R)Ft[64 + cell], (R)Ft[128 + cell], p, m);
+    Form<T>::to_double(m, p, rho, ux, uy, uz);
+  }
+  return true;
+}
+
+/* The same into slot i of Utile.  A tile outside this state's columns gets
+ * -0.0, the identity of a sum, so that adding the tiles of all slabs gives
+ * every value with its bits. */
 template <typename T, int PAR>
 __device__ __forceinline__ void tile_moments_cell(const FluidParamsT<T>& p, int tile, int i, int cell,
                                                   const double* __restrict__ Ftile, double* __restrict__ Utile) {
-  using R = typename Pop<T>::R;
-  {
-    const int tx = tile % p.ntx, ty = (tile / p.ntx) % p.nty, tz = tile / (p.ntx * p.nty);
-    const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
-    double rho = p.rho0, ux = p.ux0, uy = 0.0, uz = 0.0;
-    if (tx * 4 < p.olo || tx * 4 >= p.ohi) {
-      rho = ux = uy = uz = -0.0;
-    } else if (x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
-      const long idx = sidx(p, x, y, z);
-      R f[19];
-      load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
-      const double* Ft = Ftile + (long)i * 192;
-      Mom<R> m;
-      Form<T>::moments(f, (R)Ft[cell], (R)Ft[64 + cell], (R)Ft[128 + cell], p, m);
-      Form<T>::to_double(m, p, rho, ux, uy, uz);
-    }
-    double* U = Utile + (long)i * 256;
-    U[cell] = rho; U[64 + cell] = ux; U[128 + cell] = uy; U[192 + cell] = uz;
-  }
+  double rho, ux, uy, uz;
+  if (!tile_moment_values<T, PAR>(p, tile, i, cell, Ftile, rho, ux, uy, uz)) rho = ux = uy = uz = -0.0;
+  double* U = Utile + (long)i * 256;
+  U[cell] = rho; U[64 + cell] = ux; U[128 + cell] = uy; U[192 + cell] = uz;
 }
 
 /* Slot i of the touched-tile list: tile list[i]. */

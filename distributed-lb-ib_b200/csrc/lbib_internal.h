@@ -60,6 +60,13 @@ typedef struct lbib_device {
   long Ns;                       /* stored cells: sx * ny * nz               */
   double* halo;                  /* slab exchange buffers [4][5][ny*nz]:     */
                                  /* send_lo, send_hi, recv_lo, recv_hi       */
+  /* direct exchange: the neighbours' populations (peer or IPC-mapped device
+     pointers, with their storage geometry) and every slab's moment tiles */
+  double* peer_f[2];             /* left, right neighbour (NULL: none)       */
+  long peer_Ns[2];
+  int peer_sx[2], peer_gx0[2];
+  double* peer_U[2][8];          /* [buffer][slab], this slab's own included */
+  int npeer_U;
   int cube_size, ncx, ncy, ncz;
   int compat;
   int zin_hi;                    /* last z row the inlet/outlet copy reaches  */
@@ -145,6 +152,17 @@ int  lbdev_set_columns(lbib_device* d, int x_lo, int x_hi);
 int  lbdev_slab_pack(lbib_device* d, int par);
 int  lbdev_slab_unpack(lbib_device* d, int par);
 int  lbdev_slab_moments(lbib_device* d, double** U, long* n, int* failed_step);
+/* Direct exchange (lbdev_slab_connect first): after a fused step of parity
+ * `par`, write the face columns straight into the neighbours' storage;
+ * the moment tiles of this slab's columns into every slab's tiles. */
+int  lbdev_slab_push(lbib_device* d, int par);
+int  lbdev_slab_moments_bcast(lbib_device* d);
+int  lbdev_slab_connect(lbib_device* d, double* lo_f, long lo_Ns, int lo_sx, int lo_gx0, double* hi_f,
+                        long hi_Ns, int hi_sx, int hi_gx0, int n, double* const* U0, double* const* U1);
+int  lbdev_peer_access(int device, int peer);
+int  lbdev_ipc_handle(void* dev_ptr, void* handle);     /* 64 bytes */
+int  lbdev_ipc_open(const void* handle, void** dev_ptr);
+int  lbdev_ipc_close(void* dev_ptr);
 size_t lbdev_pop_bytes(int prec);
 /* The low-precision shift s_q and the (rho, u_x) it carries. */
 void lbdev_shift(const lbib_device* d, float* sh, double* rhos, double* uxs);

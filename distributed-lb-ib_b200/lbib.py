@@ -61,6 +61,8 @@ EXPORTED = [
     "lbib_save_restart", "lbib_load_restart", "lbib_mlp_set_stream",
     "lbib_set_slab", "lbib_case_create_slab", "lbib_slab_buffers", "lbib_slab_step_fluid",
     "lbib_slab_step_moments", "lbib_slab_moments", "lbib_slab_step_move",
+    "lbib_slab_storage", "lbib_slab_connect", "lbib_slab_step_fluid_direct", "lbib_slab_step_moments_direct",
+    "lbib_slab_check", "lbib_peer_access", "lbib_ipc_handle", "lbib_ipc_open", "lbib_ipc_close",
 ]
 
 _dp = C.POINTER(C.c_double)

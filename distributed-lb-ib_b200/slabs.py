@@ -61,6 +61,16 @@ def _bind(lib) -> None:
     for n in ("lbib_slab_step_fluid", "lbib_slab_step_moments", "lbib_slab_step_move"):
         getattr(lib, n).argtypes = [C.c_void_p]
     lib.lbib_slab_moments.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_long)]
+    vp, lp, ip = C.POINTER(C.c_void_p), C.POINTER(C.c_long), C.POINTER(C.c_int)
+    lib.lbib_slab_storage.argtypes = [C.c_void_p, vp, lp, ip, ip, vp, vp]
+    lib.lbib_slab_connect.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_int,
+                                      C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_int, vp, vp]
+    for n in ("lbib_slab_step_fluid_direct", "lbib_slab_step_moments_direct", "lbib_slab_check"):
+        getattr(lib, n).argtypes = [C.c_void_p]
+    lib.lbib_peer_access.argtypes = [C.c_int, C.c_int]
+    lib.lbib_ipc_handle.argtypes = [C.c_void_p, C.c_void_p]
+    lib.lbib_ipc_open.argtypes = [C.c_void_p, vp]
+    lib.lbib_ipc_close.argtypes = [C.c_void_p]
     lib._slab_bound = True
 
 
@@ -139,6 +149,39 @@ class SlabSolver(lbib.Solver):
     def step_move(self) -> None:
         _check(self.lib.lbib_slab_step_move(self.gv), "lbib_slab_step_move")
 
+    # ---- direct exchange (the slabs' kernels write into each other's memory)
+
+    def storage(self) -> dict:
+        """Device pointers of the populations and both moment-tile buffers,
+        and the populations' geometry (after the sheet is uploaded)."""
+        f, U0, U1 = C.c_void_p(0), C.c_void_p(0), C.c_void_p(0)
+        Ns, sx, gx0 = C.c_long(0), C.c_int(0), C.c_int(0)
+        _check(self.lib.lbib_slab_storage(self.gv, C.byref(f), C.byref(Ns), C.byref(sx), C.byref(gx0),
+                                          C.byref(U0), C.byref(U1)), "lbib_slab_storage")
+        return {"f": f.value, "Ns": Ns.value, "sx": sx.value, "gx0": gx0.value, "U0": U0.value, "U1": U1.value}
+
+    def connect(self, lo, hi, U0s, U1s) -> None:
+        """lo / hi: the neighbours' storage dicts (with "f" usable from this
+        slab's device) or None; U0s / U1s: every slab's moment-tile buffers."""
+        n = len(U0s)
+        a0 = (C.c_void_p * n)(*U0s)
+        a1 = (C.c_void_p * n)(*U1s)
+        z = {"f": None, "Ns": 0, "sx": 0, "gx0": 0}
+        lo, hi = lo or z, hi or z
+        _check(self.lib.lbib_slab_connect(self.gv, lo["f"], lo["Ns"], lo["sx"], lo["gx0"], hi["f"], hi["Ns"],
+                                          hi["sx"], hi["gx0"], n, a0, a1), "lbib_slab_connect")
+
+    def step_fluid_direct(self) -> int:
+        par = self.lib.lbib_slab_step_fluid_direct(self.gv)
+        _check(min(par, 0), "lbib_slab_step_fluid_direct")
+        return par
+
+    def step_moments_direct(self) -> None:
+        _check(self.lib.lbib_slab_step_moments_direct(self.gv), "lbib_slab_step_moments_direct")
+
+    def check(self) -> None:
+        _check(self.lib.lbib_slab_check(self.gv), "lbib_slab_check")
+
 
 def _assemble(slabs, getter):
     """Whole-grid arrays from the slabs' own columns."""
@@ -154,7 +197,7 @@ def _assemble(slabs, getter):
 class LocalSlabs:
     """All slabs of `case` in this process, slab k on device devices[k % len]."""
 
-    def __init__(self, case, n: int = 2, bounds=None, devices: Sequence[int] = (0,)):
+    def __init__(self, case, n: int = 2, bounds=None, devices: Sequence[int] = (0,), direct: bool = False):
         import torch
         self.bounds = bounds or slab_bounds(case.nx, n)
         self.devices = list(devices)
@@ -162,6 +205,17 @@ class LocalSlabs:
         for k, (lo, hi) in enumerate(self.bounds):
             with torch.cuda.device(self.devices[k % len(self.devices)]):
                 self.slabs.append(SlabSolver(case, lo, hi))
+        self.direct = direct and len(self.slabs) > 1
+        if self.direct:
+            lib = self.slabs[0].lib
+            devs = sorted(set(self.devices[:len(self.slabs)]))
+            for a in devs:
+                for b in devs:
+                    _check(lib.lbib_peer_access(a, b), "lbib_peer_access")
+            st = [s.storage() for s in self.slabs]
+            U0s, U1s = [x["U0"] for x in st], [x["U1"] for x in st]
+            for k, s in enumerate(self.slabs):
+                s.connect(st[k - 1] if k > 0 else None, st[k + 1] if k + 1 < len(st) else None, U0s, U1s)
 
     def close(self) -> None:
         for s in self.slabs:
@@ -178,6 +232,18 @@ class LocalSlabs:
         S = self.slabs
         if len(S) == 1:
             S[0].run(1)
+            return
+        if self.direct:
+            for s in S:
+                s.step_fluid_direct()
+            for s in S:
+                s.synchronize()
+            for s in S:
+                s.step_moments_direct()
+            for s in S:
+                s.check()                      # waits for the stream
+            for s in S:
+                s.step_move()
             return
         for s in S:
             s.step_fluid()
@@ -226,7 +292,7 @@ class DistSlabs:
     halo / step_fluid / step_moments / moment_tiles / step_move) so that the
     exchange logic can run without a GPU."""
 
-    def __init__(self, case=None, slab=None, bounds=None):
+    def __init__(self, case=None, slab=None, bounds=None, direct: bool = False):
         import torch.distributed as dist
         self.dist = dist
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
@@ -236,8 +302,48 @@ class DistSlabs:
             lo, hi = self.bounds[self.rank]
             slab = SlabSolver(case, lo, hi)
         self.slab = slab
+        self.direct = direct and self.world > 1
+        self._opened = []
+        if self.direct:
+            self._connect_ipc()
+
+    def _connect_ipc(self) -> None:
+        """Map the neighbours' populations and every slab's moment tiles into
+        this process (CUDA IPC) and wire the slab to them."""
+        lib = self.slab.lib
+        st = self.slab.storage()
+        def handle(ptr):
+            h = C.create_string_buffer(64)
+            _check(lib.lbib_ipc_handle(ptr, h), "lbib_ipc_handle")
+            return h.raw
+        mine = dict(st, hf=handle(st["f"]), hU0=handle(st["U0"]), hU1=handle(st["U1"]))
+        allst = [None] * self.world
+        self.dist.all_gather_object(allst, mine)
+        def open_(h):
+            p = C.c_void_p(0)
+            _check(lib.lbib_ipc_open(h, C.byref(p)), "lbib_ipc_open")
+            self._opened.append(p.value)
+            return p.value
+        U0s, U1s = [], []
+        for r, x in enumerate(allst):
+            if r == self.rank:
+                U0s.append(st["U0"]); U1s.append(st["U1"])
+            else:
+                U0s.append(open_(x["hU0"])); U1s.append(open_(x["hU1"]))
+        nb = {}
+        for side, r in (("lo", self.rank - 1), ("hi", self.rank + 1)):
+            if 0 <= r < self.world:
+                nb[side] = dict(allst[r], f=open_(allst[r]["hf"]))
+        self.slab.connect(nb.get("lo"), nb.get("hi"), U0s, U1s)
 
     def close(self) -> None:
+        if self._opened:
+            lib = self.slab.lib
+            self.dist.barrier()                # no slab writes into a mapping any more
+            for p in self._opened:
+                lib.lbib_ipc_close(p)
+            self._opened = []
+            self.dist.barrier()                # every mapping closed before any slab frees its memory
         if hasattr(self.slab, "close"):
             self.slab.close()
 
@@ -269,6 +375,15 @@ class DistSlabs:
         s, dist = self.slab, self.dist
         if getattr(s, "whole", False):         # one rank: the plain path
             s.run(1)
+            return
+        if self.direct:
+            s.step_fluid_direct()
+            s.synchronize()
+            dist.barrier()
+            s.step_moments_direct()
+            s.check()                          # waits for the stream
+            dist.barrier()
+            s.step_move()
             return
         nccl = self.backend == "nccl"
         ctx = torch.cuda.stream(torch.cuda.ExternalStream(s.stream)) if nccl else _Null()
@@ -346,12 +461,14 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--local", type=int, default=0, help="N slabs in one process on one GPU")
+    ap.add_argument("--direct", action="store_true",
+                    help="slabs write faces and moment tiles into each other's memory (peer / IPC pointers)")
     a = ap.parse_args(argv)
     case = _case(a)
     cells = a.nx * a.ny * a.nz
     out = {"lattice": [a.nx, a.ny, a.nz], "sheet": [a.rows, a.cols], "steps": a.steps, "warmup": a.warmup}
     if a.local:
-        L = LocalSlabs(case, n=a.local)
+        L = LocalSlabs(case, n=a.local, direct=a.direct)
         L.run(a.warmup)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -367,7 +484,7 @@ def main(argv=None) -> int:
             wms = (time.perf_counter() - t0) * 1e3 / a.steps
             same = bool(np.array_equal(W.sheet(), L.sheet()))
         L.close()
-        out.update(mode="local", slabs=a.local, bounds=L.bounds, ms_per_step=ms, mlups=cells / ms / 1e3,
+        out.update(mode="local", direct=bool(a.direct), slabs=a.local, bounds=L.bounds, ms_per_step=ms, mlups=cells / ms / 1e3,
                    whole_ms_per_step=wms, whole_mlups=cells / wms / 1e3, sheet_bit_identical=same)
         print(json.dumps(out))
         return 0 if same else 1
@@ -377,7 +494,7 @@ def main(argv=None) -> int:
     torch.cuda.set_device(local)
     dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                             device_id=torch.device("cuda", local))
-    D = DistSlabs(case)
+    D = DistSlabs(case, direct=a.direct)
     D.run(a.warmup)
     s = torch.cuda.ExternalStream(D.slab.stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -391,7 +508,7 @@ def main(argv=None) -> int:
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
     if D.rank == 0:
-        out.update(mode="nccl", slabs=D.world, bounds=slab_bounds(a.nx, D.world), ms_per_step=ms,
+        out.update(mode="nccl", direct=bool(a.direct), slabs=D.world, bounds=slab_bounds(a.nx, D.world), ms_per_step=ms,
                    mlups=cells / ms / 1e3)
         print(json.dumps(out))
     D.close()

@@ -328,6 +328,29 @@ int lbib_slab_step_fluid(GV gv);
 int lbib_slab_step_moments(GV gv);
 int lbib_slab_moments(GV gv, double** U, long* n);
 int lbib_slab_step_move(GV gv);
+/* Direct exchange instead of the two buffer exchanges: each slab's kernels
+ * write its face columns straight into its neighbours' populations, and its
+ * moment tiles into every slab's tiles, through device pointers that reach
+ * the other slabs' memory (peer access between GPUs of one process,
+ * lbib_peer_access; or IPC mappings between processes, lbib_ipc_*).  Wire
+ * once with lbib_slab_connect (each slab's lbib_slab_storage: populations,
+ * their geometry, both moment-tile buffers; U0/U1 list all n <= 8 slabs in
+ * order, this one included), then per step:
+ *   lbib_slab_step_fluid_direct  -> barrier over all slabs ->
+ *   lbib_slab_step_moments_direct -> barrier -> lbib_slab_check ->
+ *   lbib_slab_step_move.
+ * A barrier means: every slab's stream has finished (lbib_synchronize) and
+ * every slab knows it; no kernel here waits on another slab. */
+int lbib_slab_storage(GV gv, double** f, long* Ns, int* sx, int* gx0, double** U0, double** U1);
+int lbib_slab_connect(GV gv, double* lo_f, long lo_Ns, int lo_sx, int lo_gx0, double* hi_f, long hi_Ns,
+                      int hi_sx, int hi_gx0, int n, double* const* U0, double* const* U1);
+int lbib_slab_step_fluid_direct(GV gv);
+int lbib_slab_step_moments_direct(GV gv);
+int lbib_slab_check(GV gv);        /* waits for the stream; the step's error code */
+int lbib_peer_access(int device, int peer);
+int lbib_ipc_handle(void* dev_ptr, void* handle);          /* handle: 64 bytes */
+int lbib_ipc_open(const void* handle, void** dev_ptr);
+int lbib_ipc_close(void* dev_ptr);
 
 /* Restart files (no counterpart in the reference, which can only restart
  * from its initial state): lbib_save_restart writes everything the next

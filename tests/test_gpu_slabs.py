@@ -19,13 +19,16 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+@pytest.mark.parametrize("direct", [False, True])
 @pytest.mark.parametrize("bounds", [[(0, 20), (20, 68), (68, 128)], [(0, 64), (64, 128)]])
-def test_local_slabs_equal_whole_grid(gpu, bounds):
+def test_local_slabs_equal_whole_grid(gpu, bounds, direct):
+    """direct: the slabs' kernels write faces and moment tiles straight into
+    each other's memory; otherwise through the face buffers and a sum."""
     case, steps = c0_case(), 25
     with lbib.Solver(case) as whole:
         whole.run(steps)
         sheet, df1, mom = whole.sheet(), whole.df1(), whole.moments()
-    with slabs.LocalSlabs(case, bounds=bounds) as L:
+    with slabs.LocalSlabs(case, bounds=bounds, direct=direct) as L:
         L.run(steps)
         assert np.array_equal(L.sheet(), sheet)
         assert np.array_equal(L.df1()[:, 2:-2, 2:-2, 2:-2], df1[:, 2:-2, 2:-2, 2:-2])
@@ -58,7 +61,7 @@ def _slab_case():
     return small_case(64, 16, 16, 8, 8, x0=30.0)
 
 
-def _rank_main(rank, world, port, steps, q):
+def _rank_main(rank, world, port, steps, q, direct=False):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     for p in (os.path.join(ROOT, "distributed-lb-ib_b200"), os.path.join(ROOT, "tests"),
               os.path.join(ROOT, "oracle")):
@@ -67,7 +70,7 @@ def _rank_main(rank, world, port, steps, q):
     import torch.distributed as dist
     import slabs as S
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
-    d = S.DistSlabs(case=_slab_case())
+    d = S.DistSlabs(case=_slab_case(), direct=direct)
     d.run(steps)
     s = d.slab
     q.put((rank, s.x_lo, s.x_hi, s.sheet(), s.df1()[:, :, :, s.columns]))
@@ -76,7 +79,11 @@ def _rank_main(rank, world, port, steps, q):
     dist.destroy_process_group()
 
 
-def test_two_ranks_gloo_equal_whole_grid(gpu):
+@pytest.mark.parametrize("direct", [False, True])
+def test_two_ranks_gloo_equal_whole_grid(gpu, direct):
+    """Two processes on one GPU: face buffers through gloo, or (direct) each
+    rank's kernels writing into the other's memory through CUDA IPC, with a
+    host barrier between the phases (no kernel waits on the other rank)."""
     steps, world = 31, 2
     case = _slab_case()
     with lbib.Solver(case) as whole:
@@ -85,7 +92,7 @@ def test_two_ranks_gloo_equal_whole_grid(gpu):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, steps, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, steps, q, direct)) for r in range(world)]
     for p in procs:
         p.start()
     out = [q.get(timeout=300) for _ in procs]
