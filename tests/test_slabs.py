@@ -43,9 +43,15 @@ def test_slab_arguments_checked_before_any_gpu_call(lbib_built):
     n = ctypes.c_long(0)
     assert lib.lbib_slab_buffers(None, bufs, ctypes.byref(n)) == -1
     lib.lbib_clear_error()
-    for f in ("lbib_slab_step_fluid", "lbib_slab_step_moments", "lbib_slab_step_move"):
+    for f in ("lbib_slab_step_fluid", "lbib_slab_step_moments", "lbib_slab_step_move",
+              "lbib_slab_step_fluid_direct", "lbib_slab_step_moments_direct"):
         assert getattr(lib, f)(None) == -1
         lib.lbib_clear_error()
+    a = (ctypes.c_void_p * 1)(None)
+    assert lib.lbib_slab_connect(None, None, 0, 0, 0, None, 0, 0, 0, 1, a, a) == -1
+    assert lib.lbib_ipc_handle(None, None) == -1 and lib.lbib_ipc_open(None, None) == -1
+    assert lib.lbib_ipc_close(None) == -1
+    lib.lbib_clear_error()
 
 
 def _free_port():
