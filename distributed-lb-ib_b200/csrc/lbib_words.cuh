@@ -399,17 +399,19 @@ __device__ __forceinline__ void edge_cell(const FluidParamsT<T>& p, int nry, int
 /* The word-kernel variants that the one-grid and the batched launches and
  * their autotuners choose from: {cells per thread V, resident blocks per SM
  * the registers are sized for}.  16-bit storage: {4,3} {4,4} {2,4} {2,5}
- * {2,6}; FP32: {2,3} {2,4} {2,5}.  (A variant that prefetched the next rows'
+ * {2,6} {4,5} (the last spills ~64 bytes and still measured fastest at
+ * 512x256x256: occupancy buys more than the spills cost); FP32: {2,3}
+ * {2,4} {2,5}.  (A variant that prefetched the next rows'
  * words into shared memory with cp.async measured no faster and was
  * dropped.)  with_variant calls f(V, MINB) as integral constants. */
-constexpr int kWordVariants16 = 5, kWordVariants32 = 3;
+constexpr int kWordVariants16 = 6, kWordVariants32 = 3;
 
 __host__ __forceinline__ int word_variants(int prec) {
   return LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? kWordVariants32 : kWordVariants16;
 }
 
 __host__ __forceinline__ int word_variant_cells(int prec, int v) {
-  return LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? 2 : (v <= 1 ? 4 : 2);
+  return LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? 2 : ((v <= 1 || v == 5) ? 4 : 2);
 }
 
 template <typename T, typename F>
@@ -421,6 +423,7 @@ int with_variant(int v, F&& f) {
       case 2: return f(integral_constant<int, 2>{}, integral_constant<int, 4>{});
       case 3: return f(integral_constant<int, 2>{}, integral_constant<int, 5>{});
       case 4: return f(integral_constant<int, 2>{}, integral_constant<int, 6>{});
+      case 5: return f(integral_constant<int, 4>{}, integral_constant<int, 5>{});
       default: return f(integral_constant<int, 4>{}, integral_constant<int, 3>{});
     }
   } else {
