@@ -459,14 +459,27 @@ __device__ __forceinline__ void move_node(double* __restrict__ nodes, const doub
   const double c_64 = 1.0 / (6.4e1);
   const int is = st[i * 3 + 0], js = st[i * 3 + 1], ks = st[i * 3 + 2];
   const double* w = W + i * 12;
+  /* the stencil spans at most 2 tiles per axis: look their slots up first,
+     so that the 64 cells' loads below do not wait on one another */
+  const int tx0 = is >> 2, ty0 = js >> 2, tz0 = ks >> 2;
+  int sp8[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int tx = tx0 + (a & 1), ty = ty0 + ((a >> 1) & 1), tz = tz0 + (a >> 2);
+    const bool need = tx * 4 <= is + 3 && ty * 4 <= js + 3 && tz * 4 <= ks + 3;
+    sp8[a] = need ? slot[(tz * nty + ty) * ntx + tx] : 0;
+  }
   double s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
   for (int i2 = 0; i2 <= 3; i2++) {
     const int gi = is + i2;
+#pragma unroll
     for (int j2 = 0; j2 <= 3; j2++) {
       const int gj = js + j2;
+#pragma unroll
       for (int k2 = 0; k2 <= 3; k2++) {
         const int gk = ks + k2;
-        const int sp = slot[lbib::tile_of(gi, gj, gk, ntx, nty)];
+        const int sp = sp8[((gi >> 2) - tx0) | (((gj >> 2) - ty0) << 1) | (((gk >> 2) - tz0) << 2)];
         const double* U = Utile + (long)sp * 256;
         const int cell = lbib::cell_in_tile(gi, gj, gk);
         const double vx = U[64 + cell], vy = U[128 + cell], vz = U[192 + cell];
