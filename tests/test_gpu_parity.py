@@ -61,7 +61,7 @@ EXTRA_CASES = {
 
 @pytest.fixture(params=["staged", "generic"])
 def fluid_path(request, monkeypatch):
-    """Rows away from the walls run the bulk-copy staged kernel unless
+    """Rows away from the walls run the two-cell kernel unless
     LBIB_FLUID_BULK=0; both paths must give the same bits."""
     if request.param == "generic":
         monkeypatch.setenv("LBIB_FLUID_BULK", "0")
