@@ -130,7 +130,7 @@ static int build_rows(lbib_device* d) {
      FP64 two-cell kernel wants even nx */
   const int v = LBIB_PREC_TYPE(d->prec) == LBIB_PREC_F64 ? 2 : (int)(8 / lbdev_pop_bytes(d->prec));
   d->use_bulk = !(env && env[0] == '0') && (d->nx % v == 0) && lbdev_bulk_rows(d, &ry, &rz);
-  const int zb = 2 + rz;  /* last z row of the staged kernel */
+  const int zb = 2 + rz;  /* last z row of the bulk kernels */
   long cap = (long)(d->ny - 4) * (d->nz - 4);
   int* h = (int*)malloc(sizeof(int) * 2 * cap);
   if (!h) return -5;

@@ -59,7 +59,7 @@ EXTRA_CASES = {
 }
 
 
-@pytest.fixture(params=["staged", "generic"])
+@pytest.fixture(params=["two_cell", "generic"])
 def fluid_path(request, monkeypatch):
     """Rows away from the walls run the two-cell kernel unless
     LBIB_FLUID_BULK=0; both paths must give the same bits."""
