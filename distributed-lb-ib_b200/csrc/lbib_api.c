@@ -32,7 +32,7 @@ const char* lbib_error_string(int code) {
     case LBIB_E_ARG: return "invalid argument (size, NULL pointer or indivisible grid)";
     case LBIB_E_CUDA: return "a CUDA call failed";
     case LBIB_E_STENCIL: return "a fiber node's 4x4x4 stencil left the fluid grid";
-    case LBIB_E_STATE: return "call out of order (no grid, sheet or initial state yet)";
+    case LBIB_E_STATE: return "call out of order (no grid, sheet or initial state yet), or not for this grid (a slab / the whole grid)";
     case LBIB_E_NOMEM: return "allocation failed";
     case LBIB_E_CAPACITY: return "touched-tile capacity exceeded";
     case LBIB_E_IO: return "a dump file could not be written";

@@ -38,6 +38,30 @@ def test_local_slabs_equal_whole_grid(gpu, bounds, direct):
         assert np.abs(sheet[..., 0] - L.slabs[0].case.sheets[0].x0).max() > 0
 
 
+def test_slab_refuses_the_whole_grid_calls(gpu, tmp_path):
+    """A slab GV cannot run whole-grid steps or write restart files; a whole
+    grid cannot take slab steps."""
+    case = small_case(64, 16, 16, 8, 8, x0=30.0)
+    s = slabs.SlabSolver(case, 0, 32)
+    try:
+        with pytest.raises(lbib.LbibError, match="out of order"):
+            s.run(1)
+        with pytest.raises(lbib.LbibError, match="out of order"):
+            s.save(str(tmp_path / "r.bin"))
+        with pytest.raises(lbib.LbibError, match="out of order"):
+            s.step_fluid_direct()                      # not connected
+    finally:
+        s.close()
+    w = slabs.SlabSolver(case, 0, 64)                  # the whole grid
+    try:
+        assert w.whole
+        with pytest.raises(lbib.LbibError, match="out of order"):
+            w.step_fluid()
+        w.run(2)
+    finally:
+        w.close()
+
+
 def test_a_stencil_leaving_the_grid_stops_the_slabs(gpu):
     # a sheet one cell from the outlet: its stencil leaves the grid within a few steps
     bad = Case(32, 16, 16, [Sheet(4, 4, 1.5, 1.5, 29.3, 7.0, 7.0)], u_l=0.1)
