@@ -212,8 +212,6 @@ struct lbib_batch {
   long nrblk;
   int2* xblk;                    /* FP64 two-cell blocks (problem, block) */
   long nxblk;
-  int2* eblk;                    /* edge-cell blocks (problem, first bulk row) */
-  long neblk;
   int* variant;                  /* word-kernel variant per problem */
   int2* wblk[MAXV];              /* word blocks of each variant group */
   long nwblk[MAXV];
@@ -314,12 +312,12 @@ int build_word_blocks(lbib_batch* b) {
 }
 
 /* Rows of the generic kernel (every row of I for problems without bulk
- * rows; the wall rows otherwise) and their 128-cell blocks; the bulk rows'
- * blocks: FP64 two-cell blocks, or the edge-cell blocks of the
- * low-precision word kernel (whose own blocks build_word_blocks makes). */
+ * rows; the wall rows otherwise) and their 128-cell blocks, and the FP64
+ * two-cell blocks of the bulk rows (the low-precision word blocks, which
+ * also step the plane-adjacent cells, come from build_word_blocks). */
 int build_rows(lbib_batch* b) {
   const int lp = is_lp(b);
-  long n = 0, nr = 0, ne = 0, nxb = 0;
+  long n = 0, nr = 0, nxb = 0;
   for (int k = 0; k < b->B; ++k) {
     const lbib_device* d = b->sh[k];
     int ry = 0, rz = 0;
@@ -327,15 +325,13 @@ int build_rows(lbib_batch* b) {
     const long rows = (long)(d->ny - 4) * (d->nz - 4) - (bulk ? (long)ry * rz : 0);
     n += rows;
     nr += (rows * (d->nx - 4) + 127) / 128;
-    if (bulk && lp) ne += ((long)ry * rz + 31) / 32;
     if (bulk && !lp) nxb += ((long)ry * rz * ((d->nx - 4) / 2) + 127) / 128;
   }
   int2* h = (int2*)malloc(sizeof(int2) * (n ? n : 1));
   int4* rb = (int4*)malloc(sizeof(int4) * (nr ? nr : 1));
-  int2* eo = (int2*)malloc(sizeof(int2) * (ne ? ne : 1));
   int2* xo = (int2*)malloc(sizeof(int2) * (nxb ? nxb : 1));
-  if (!h || !rb || !eo || !xo) { free(h); free(rb); free(eo); free(xo); return -5; }
-  long r = 0, ir = 0, ie = 0, ix = 0;
+  if (!h || !rb || !xo) { free(h); free(rb); free(xo); return -5; }
+  long r = 0, ir = 0, ix = 0;
   for (int k = 0; k < b->B; ++k) {
     const lbib_device* d = b->sh[k];
     int ry = 0, rz = 0;
@@ -349,26 +345,20 @@ int build_rows(lbib_batch* b) {
       }
     const long rows = r - r0;
     for (long j = 0; j < (rows * (d->nx - 4) + 127) / 128; ++j) rb[ir++] = make_int4(k, (int)r0, (int)rows, (int)j);
-    if (bulk && lp)
-      for (long q = 0; q < (long)ry * rz; q += 32) eo[ie++] = make_int2(k, (int)q);
     if (bulk && !lp)
       for (long j = 0; j < ((long)ry * rz * ((d->nx - 4) / 2) + 127) / 128; ++j) xo[ix++] = make_int2(k, (int)j);
   }
   b->nrblk = nr;
-  b->neblk = ne;
   b->nxblk = nxb;
   int rc = 0;
   if (cudaMalloc(&b->rowyz, sizeof(int2) * (n ? n : 1)) != cudaSuccess) rc = -5;
   else if (n && cudaMemcpy(b->rowyz, h, sizeof(int2) * n, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
   if (!rc && cudaMalloc(&b->rblk, sizeof(int4) * (nr ? nr : 1)) != cudaSuccess) rc = -5;
   else if (!rc && nr && cudaMemcpy(b->rblk, rb, sizeof(int4) * nr, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
-  if (!rc && cudaMalloc(&b->eblk, sizeof(int2) * (ne ? ne : 1)) != cudaSuccess) rc = -5;
-  else if (!rc && ne && cudaMemcpy(b->eblk, eo, sizeof(int2) * ne, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
   if (!rc && cudaMalloc(&b->xblk, sizeof(int2) * (nxb ? nxb : 1)) != cudaSuccess) rc = -5;
   else if (!rc && nxb && cudaMemcpy(b->xblk, xo, sizeof(int2) * nxb, cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
   free(h);
   free(rb);
-  free(eo);
   free(xo);
   return rc;
 }
@@ -387,8 +377,6 @@ BatchFluid fluid_args(lbib_batch* b, int par, const void* P, const void* WP, int
   f.nrblk = b->nrblk;
   f.xblk = b->xblk;
   f.nxblk = b->nxblk;
-  f.eblk = b->eblk;
-  f.neblk = b->neblk;
   f.list = b->tile_list[c];
   f.count = b->tile_count[c];
   f.tile_inst = b->tile_inst;
@@ -439,7 +427,7 @@ int batch_step(lbib_batch* b) {
         b->launches++;
       }
     if (batch_fluid_rest_lp(f)) return -2;
-    b->launches += 1 + (b->nrblk > 0) + (b->neblk > 0);
+    b->launches += 1 + (b->nrblk > 0);
   } else {
     if (batch_fluid_rest_f64(f)) return -2;
     b->launches += (b->nxblk > 0) + (b->nrblk > 0);
@@ -721,7 +709,7 @@ void lbib_batch_free(lbib_batch* b) {
   cudaFree(b->err);
   cudaFree(b->step_no);
   if (b->h_err) cudaFreeHost(b->h_err);
-  cudaFree(b->desc); cudaFree(b->rowyz); cudaFree(b->rblk); cudaFree(b->eblk); cudaFree(b->xblk);
+  cudaFree(b->desc); cudaFree(b->rowyz); cudaFree(b->rblk); cudaFree(b->xblk);
   for (int v = 0; v < MAXV; ++v) cudaFree(b->wblk[v]);
   if (b->stream) cudaStreamDestroy(b->stream);
   free(b->prob); free(b->h_desc); free(b->variant);

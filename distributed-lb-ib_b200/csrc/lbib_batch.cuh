@@ -11,8 +11,8 @@
  *            each problem's rows laid end to end;
  *   pairs    (FP64) blocks of 128 cell pairs of the two-cell kernel;
  *   words    blocks of the word kernel, (problem, block within problem);
- *   edges    (low precision) the cells x in {2, 3, nx-4, nx-3} of bulk
- *            rows, blocks of (problem, 32 rows);
+ *            (the word blocks also step the cells x in {2, 3, nx-4, nx-3}
+ *            of the rows whose first word they hold);
  *   tiles    the global touched-tile list, tile -> problem by a table.
  * A problem whose error word is set (a fiber stencil left its grid) is
  * skipped by every kernel from then on; the others continue.
@@ -68,7 +68,13 @@ __global__ void __launch_bounds__(128) lbib_b_rows(const FluidParamsT<T>* __rest
   step_cell<T, PAR>(sp, 2 + c % w, yz.x, yz.y);
 }
 
-/* Word kernel over the blocks of all problems that run it. */
+/* Word kernel over the blocks of all problems that run it.  A block also
+ * steps the plane-adjacent cells x in {2, 3, nx-4, nx-3} of the rows whose
+ * first word it holds (generic per-cell rules), right after their words
+ * went through the caches: a launch of their own re-read each of their
+ * 2-byte populations from DRAM as a whole sector.  The slots those cells
+ * read and write are theirs alone (AA), so the order within the launch
+ * does not matter. */
 template <typename T, int V, int PAR, int MINB>
 __global__ void __launch_bounds__(WTPB, MINB) lbib_b_words(const WordsParams<T>* __restrict__ WP,
                                                            const int2* __restrict__ blk, const int* __restrict__ err) {
@@ -76,21 +82,12 @@ __global__ void __launch_bounds__(WTPB, MINB) lbib_b_words(const WordsParams<T>*
   const int2 m = blk[blockIdx.x];
   if (err[2 * m.x]) return;
   block_copy(sb, WP + m.x);
-  words_item<T, V, PAR>(sb, (long)m.y * WTPB + threadIdx.x);
-}
-
-/* Edge cells: a block per (problem, 32 bulk rows), 4 cells per row. */
-template <typename T, int PAR>
-__global__ void __launch_bounds__(128) lbib_b_edges(const FluidParamsT<T>* __restrict__ P,
-                                                    const WordsParams<T>* __restrict__ WP,
-                                                    const int2* __restrict__ blk, const int* __restrict__ err) {
-  __shared__ __align__(16) FluidParamsT<T> sp;
-  const int2 m = blk[blockIdx.x];
-  if (err[2 * m.x]) return;
-  block_copy(sp, P + m.x);
-  const int r = m.y + (int)(threadIdx.x >> 2);
-  if (r >= WP[m.x].nrows) return;
-  edge_cell<T, PAR>(sp, WP[m.x].nry, r, threadIdx.x & 3);
+  const long first = (long)m.y * WTPB;
+  words_item<T, V, PAR>(sb, first + threadIdx.x);
+  const long r0 = (first + sb.gpr - 1) / sb.gpr;
+  long r1 = (first + WTPB + sb.gpr - 1) / sb.gpr;
+  if (r1 > sb.nrows) r1 = sb.nrows;
+  for (long i = threadIdx.x; i < 4 * (r1 - r0); i += WTPB) edge_cell<T, PAR>(sb.p, sb.nry, (int)(r0 + i / 4), (int)(i & 3));
 }
 
 /* Cells of forced tiles in the word kernel's range, over the global list. */

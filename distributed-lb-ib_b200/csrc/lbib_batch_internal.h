@@ -26,8 +26,6 @@ struct BatchFluid {
   long nrblk;
   const int2* xblk;        /* FP64 two-cell blocks: (problem, block) */
   long nxblk;
-  const int2* eblk;        /* edge-cell blocks: (problem, first bulk row) */
-  long neblk;
   const int* list;         /* touched tiles (global ids) */
   const int* count;
   const int* tile_inst;
@@ -37,7 +35,7 @@ struct BatchFluid {
   int grid_tiles;          /* persistent grid for tile-list kernels */
 };
 
-/* Generic rows + edge cells + forced cells (the word blocks are separate);
+/* Generic rows + forced cells (the word blocks, with the edge cells, are separate);
  * FP64: two-cell blocks + generic rows. */
 int batch_fluid_rest_f64(const BatchFluid& f);
 int batch_fluid_rest_lp(const BatchFluid& f);

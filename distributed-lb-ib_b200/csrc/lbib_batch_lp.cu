@@ -13,14 +13,9 @@ namespace {
 template <typename T>
 int rest(const BatchFluid& f) {
   const FluidParamsT<T>* P = static_cast<const FluidParamsT<T>*>(f.P);
-  const WordsParams<T>* WP = static_cast<const WordsParams<T>*>(f.WP);
   if (f.nrblk > 0) {
     if (f.par == 0) lbib_b_rows<T, 0><<<(unsigned)f.nrblk, 128, 0, f.stream>>>(P, f.rowyz, f.rblk, f.err);
     else lbib_b_rows<T, 1><<<(unsigned)f.nrblk, 128, 0, f.stream>>>(P, f.rowyz, f.rblk, f.err);
-  }
-  if (f.neblk > 0) {
-    if (f.par == 0) lbib_b_edges<T, 0><<<(unsigned)f.neblk, 128, 0, f.stream>>>(P, WP, f.eblk, f.err);
-    else lbib_b_edges<T, 1><<<(unsigned)f.neblk, 128, 0, f.stream>>>(P, WP, f.eblk, f.err);
   }
   if (f.par == 0) lbib_b_forced<T, 0><<<f.grid_tiles, 64, 0, f.stream>>>(P, f.desc, f.list, f.count, f.tile_inst, f.err);
   else lbib_b_forced<T, 1><<<f.grid_tiles, 64, 0, f.stream>>>(P, f.desc, f.list, f.count, f.tile_inst, f.err);
