@@ -26,7 +26,15 @@ namespace {
 
 template <typename T, int V, int PAR, int MINB>
 __global__ void __launch_bounds__(WTPB, MINB) lbib_fluid_step_words(WordsParams<T> b) {
-  words_item<T, V, PAR>(b, (long)blockIdx.x * WTPB + threadIdx.x);
+  const long first = (long)blockIdx.x * WTPB;
+  words_item<T, V, PAR>(b, first + threadIdx.x);
+  /* the plane-adjacent cells x in {2, 3, nx-4, nx-3} of the rows whose first
+     word this block holds, while their words are in the caches (their slots
+     are theirs alone, so the order within the launch does not matter) */
+  const long r0 = (first + b.gpr - 1) / b.gpr;
+  long r1 = (first + WTPB + b.gpr - 1) / b.gpr;
+  if (r1 > b.nrows) r1 = b.nrows;
+  for (long i = threadIdx.x; i < 4 * (r1 - r0); i += WTPB) edge_cell<T, PAR>(b.p, b.nry, (int)(r0 + i / 4), (int)(i & 3));
 }
 
 /* Cells of this step's forced tiles inside the word kernel's range; a
@@ -36,14 +44,6 @@ __global__ void __launch_bounds__(64) lbib_forced_cells(FluidParamsT<T> p, const
                                                         const int* __restrict__ count, int zb) {
   const int n = *count;
   for (int i = blockIdx.x; i < n; i += gridDim.x) forced_cell<T, PAR>(p, list[i], threadIdx.x, zb);
-}
-
-/* Cells x in {2, 3, nx-4, nx-3} of the bulk rows. */
-template <typename T, int PAR>
-__global__ void __launch_bounds__(128) lbib_edge_cells(FluidParamsT<T> p, int nry, int nrows) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 4 * nrows) return;
-  edge_cell<T, PAR>(p, nry, i >> 2, i & 3);
 }
 
 int sm_count() {
@@ -66,19 +66,16 @@ int launch_words(lbib_device* d, const FluidParamsT<T>& p) {
   words_geometry(b, V, d->nx, nry, nrz);
   const long threads = b.nrows * b.gpr;
   const unsigned blocks = (unsigned)((threads + WTPB - 1) / WTPB);
-  const unsigned eblocks = (unsigned)((4 * b.nrows + 127) / 128);
   const int zb = 2 + nrz, c = d->cur;
   const unsigned fblocks = (unsigned)sm_count() * 8;
   if (d->parity == 0) {
     lbib_fluid_step_words<T, V, 0, MINB><<<blocks, WTPB, 0, d->stream>>>(b);
-    lbib_edge_cells<T, 0><<<eblocks, 128, 0, d->stream>>>(p, b.nry, (int)b.nrows);
     lbib_forced_cells<T, 0><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
   } else {
     lbib_fluid_step_words<T, V, 1, MINB><<<blocks, WTPB, 0, d->stream>>>(b);
-    lbib_edge_cells<T, 1><<<eblocks, 128, 0, d->stream>>>(p, b.nry, (int)b.nrows);
     lbib_forced_cells<T, 1><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
   }
-  d->kernel_launches += 3;
+  d->kernel_launches += 2;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

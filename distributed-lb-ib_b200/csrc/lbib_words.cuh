@@ -18,8 +18,10 @@
  * read and written only by the cell that pushes into it keeps that
  * race-free.  Groups whose tile carries force this step, and the cells
  * x in {2, 3, nx-4, nx-3}, are left to the generic per-cell rules
- * (forced_cell / edge_cell below); their words are still loaded by idle
- * lanes so the shuffles see them, and no two kernels write the same element.
+ * (forced_cell in a launch of its own; edge_cell, run by the word blocks
+ * after their words for the rows whose first word they hold); their words
+ * are still loaded by idle lanes so the shuffles see them, and no two
+ * threads write the same element.
  */
 #ifndef LBIB_WORDS_CUH
 #define LBIB_WORDS_CUH
