@@ -213,6 +213,8 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   if (rc) { lbdev_free(d); return rc; }
   d->cur = 0;
   d->lp_variant = -1;
+  const char* pf = getenv("LBIB_L2_PREFETCH");
+  d->l2_pf = pf ? atoi(pf) : 0;
   *out = d;
   return 0;
 }

@@ -27,6 +27,7 @@ namespace {
 template <typename T, int V, int PAR, int MINB>
 __global__ void __launch_bounds__(WTPB, MINB) lbib_fluid_step_words(WordsParams<T> b) {
   const long first = (long)blockIdx.x * WTPB;
+  if (b.pf > 0) words_prefetch<T, V, PAR>(b, blockIdx.x + b.pf);
   words_item<T, V, PAR>(b, first + threadIdx.x);
   /* the plane-adjacent cells x in {2, 3, nx-4, nx-3} of the rows whose first
      word this block holds, while their words are in the caches (their slots
@@ -64,6 +65,7 @@ int launch_words(lbib_device* d, const FluidParamsT<T>& p) {
   int nry = 0, nrz = 0;
   if (!lbdev_bulk_rows(d, &nry, &nrz)) return 0;
   words_geometry(b, V, d->nx, nry, nrz);
+  b.pf = (long)d->l2_pf * sm_count() * MINB;
   const long threads = b.nrows * b.gpr;
   const unsigned blocks = (unsigned)((threads + WTPB - 1) / WTPB);
   const int zb = 2 + nrz, c = d->cur;

@@ -148,6 +148,13 @@ __device__ __forceinline__ void fiber_forces_node(double* __restrict__ nodes, in
 
 __device__ __forceinline__ int stencil_start(double p) { return (int)(floor(p / 1.0 - 2) + 1); }
 
+/* The stencil of a node at coordinate p lies inside an axis of n cells:
+ * start = floor(p - 2) + 1 in [0, n - 4], i.e. 1 <= p < n - 2, decided on
+ * the double itself so that NaN and huge coordinates fail the test (the
+ * reference stops with "out of bound" there; an int conversion first would
+ * turn NaN into 0 and pass). */
+__device__ __forceinline__ bool stencil_inside(double p, int n) { return p >= 1.0 && p < (double)n - 2.0; }
+
 /* Node i: stencil start, the twelve delta-kernel factors, a count for every
  * 4^3 tile its stencil touches (tile ids offset by tile0); b0..b5 receive
  * its stencil box (left empty when the stencil leaves the grid). */
@@ -157,7 +164,9 @@ __device__ __forceinline__ void node_prep_one(const double* __restrict__ nodes, 
                                               int& b0, int& b1, int& b2, int& b3, int& b4, int& b5) {
   {
     const double* m = nodes + i * 12;
-    const int is = stencil_start(m[0]), js = stencil_start(m[1]), ks = stencil_start(m[2]);
+    const bool inside = stencil_inside(m[0], nx) && stencil_inside(m[1], ny) && stencil_inside(m[2], nz);
+    const int is = inside ? stencil_start(m[0]) : 0, js = inside ? stencil_start(m[1]) : 0,
+              ks = inside ? stencil_start(m[2]) : 0;
     st[i * 3 + 0] = is; st[i * 3 + 1] = js; st[i * 3 + 2] = ks;
     const double cxk = kPi / (2.0 * 1.0);
     double* w = W + i * 12;
@@ -166,7 +175,7 @@ __device__ __forceinline__ void node_prep_one(const double* __restrict__ nodes, 
       w[4 + a] = 1.0e0 + lbib_cos(cxk * (1.0 * (js + a) - m[1]));
       w[8 + a] = 1.0e0 + lbib_cos(cxk * (1.0 * (ks + a) - m[2]));
     }
-    if (is < 0 || is + 3 >= nx || js < 0 || js + 3 >= ny || ks < 0 || ks + 3 >= nz) {
+    if (!inside) {
       set_error(err, -3, step);
     } else {
       for (int tz = ks >> 2; tz <= (ks + 3) >> 2; ++tz)

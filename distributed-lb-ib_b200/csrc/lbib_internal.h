@@ -86,6 +86,8 @@ typedef struct lbib_device {
   long steps;                    /* fused steps since init_df1               */
   int use_bulk;                  /* bulk kernel for rows away from walls     */
   int lp_variant;                /* low-precision word-kernel variant, -1 = default */
+  int l2_pf;                     /* bulk kernels: L2 prefetch distance, in waves of
+                                    resident blocks (0: none)                  */
   int* rows;                     /* device int2 (y, z) rows of the generic kernel */
   int nrows;
   int have_eq, have_df1, have_inout;

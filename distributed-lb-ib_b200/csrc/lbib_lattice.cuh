@@ -159,6 +159,21 @@ __device__ __forceinline__ long link_offset(int q, long sy, long sz) {
   return (long)cx(q) + (long)cy(q) * sy + (long)cz(q) * sz;
 }
 
+/* Ask L2 to fetch the bytes [lo, hi) of the buffer [base, end) ahead of
+ * their loads (cp.async.bulk.prefetch, sm_90+): the range is widened to
+ * 16-byte boundaries, as the instruction requires, and clipped to the
+ * buffer.  A hint only -- no register holds the data and nothing waits on
+ * it -- so a fused step can keep more DRAM traffic in flight than its
+ * resident warps' loads alone. */
+__device__ __forceinline__ void l2_prefetch(const void* lo, const void* hi, const void* base, const void* end) {
+  uintptr_t a = (uintptr_t)lo & ~(uintptr_t)15;
+  uintptr_t b = ((uintptr_t)hi + 15) & ~(uintptr_t)15;
+  const uintptr_t a0 = ((uintptr_t)base + 15) & ~(uintptr_t)15, b0 = (uintptr_t)end & ~(uintptr_t)15;
+  if (a < a0) a = a0;
+  if (b > b0) b = b0;
+  if (b > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(b - a)) : "memory");
+}
+
 /* Pre-collision populations of cell (x, y, z) in I for a step of parity PAR. */
 template <int PAR, typename T>
 __device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y, int z, long idx, int kind,

@@ -42,6 +42,11 @@ constexpr double kPiNa = 3.14159265358979;  /* the reference's truncated PI */
 
 __device__ __forceinline__ int na_start(double p) { return (int)(floor(p / 1.0 - 2) + 1); }
 
+/* start = floor(p - 2) + 1 in [0, n - 4] <=> 1 <= p < n - 2, tested on the
+ * double so that NaN and huge coordinates are rejected before any int
+ * conversion. */
+__device__ __forceinline__ bool na_inside(double p, int n) { return p >= 1.0 && p < (double)n - 2.0; }
+
 /* Everything that must start a call at a known value. */
 __global__ void na_clear(int* s) {
   s[0] = INT_MAX; s[1] = INT_MIN; s[2] = INT_MAX; s[3] = INT_MIN; s[4] = INT_MAX; s[5] = INT_MIN;
@@ -55,10 +60,10 @@ __global__ void na_boxes(const double* __restrict__ nodes, long S, int nx, int n
   int b0 = INT_MAX, b1 = INT_MIN, b2 = INT_MAX, b3 = INT_MIN, b4 = INT_MAX, b5 = INT_MIN;
   if (i < S) {
     const double* m = nodes + i * 12;
-    const int is = na_start(m[0]), js = na_start(m[1]), ks = na_start(m[2]);
-    if (is < 0 || is + 3 >= nx || js < 0 || js + 3 >= ny || ks < 0 || ks + 3 >= nz) {
+    if (!(na_inside(m[0], nx) && na_inside(m[1], ny) && na_inside(m[2], nz))) {
       atomicCAS(&s[6], 0, LBIB_E_STENCIL);
     } else {
+      const int is = na_start(m[0]), js = na_start(m[1]), ks = na_start(m[2]);
       b0 = is; b1 = is + 3; b2 = js; b3 = js + 3; b4 = ks; b5 = ks + 3;
     }
   }
@@ -153,19 +158,16 @@ __global__ void __launch_bounds__(64) na_gather(const double* __restrict__ nodes
   }
 }
 
-/* Device address of lbib_noalloc_scratch, looked up once per device with
- * that device current. */
-int* g_scratch_addr[64];
-
+/* Device address of lbib_noalloc_scratch in the current device's context.
+ * Looked up on every call (no cache): after a cudaDeviceReset, or under
+ * another context on the same device ordinal, the module is loaded anew and
+ * an address kept from before would point at freed memory.  The lookup
+ * allocates nothing once the module is loaded (the first call on a device
+ * loads it). */
 int scratch_for_current_device(int** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return LBIB_E_CUDA;
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, lbib_noalloc_scratch) != cudaSuccess || !p) return LBIB_E_CUDA;
-    g_scratch_addr[dev] = (int*)p;
-  }
-  *out = g_scratch_addr[dev];
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, lbib_noalloc_scratch) != cudaSuccess || !p) return LBIB_E_CUDA;
+  *out = (int*)p;
   return LBIB_OK;
 }
 
@@ -175,6 +177,9 @@ extern "C" int lbib_spread_force_noalloc(const double* nodes, long num_nodes, in
                                          double* fy, double* fz, void* stream) {
   if (!nodes || !fx || !fy || !fz || num_nodes < 1 || nx < 4 || ny < 4 || nz < 4) return LBIB_E_ARG;
   if (num_nodes > LBIB_NOALLOC_MAX_NODES) return LBIB_E_LIMIT;
+  /* a launch error left by earlier, unrelated work is not this call's:
+     refuse to run on it rather than report it as ours */
+  if (cudaPeekAtLastError() != cudaSuccess) return LBIB_E_CUDA;
   int* s = nullptr;
   int rc = scratch_for_current_device(&s);
   if (rc) return rc;
@@ -182,11 +187,13 @@ extern "C" int lbib_spread_force_noalloc(const double* nodes, long num_nodes, in
   const long N = (long)nx * ny * nz;
   const long nchunks = (num_nodes + 31) / 32;
   na_clear<<<1, 1, 0, st>>>(s);
+  if (cudaGetLastError() != cudaSuccess) return LBIB_E_CUDA;
   if (cudaMemsetAsync(fx, 0, sizeof(double) * N, st) != cudaSuccess ||
       cudaMemsetAsync(fy, 0, sizeof(double) * N, st) != cudaSuccess ||
       cudaMemsetAsync(fz, 0, sizeof(double) * N, st) != cudaSuccess)
     return LBIB_E_CUDA;
   na_boxes<<<(unsigned)((num_nodes + 127) / 128), 128, 0, st>>>(nodes, num_nodes, nx, ny, nz, s);
+  if (cudaGetLastError() != cudaSuccess) return LBIB_E_CUDA;
   na_gather<<<148 * 8, 64, 0, st>>>(nodes, num_nodes, nchunks, nx, ny, nz, s, fx, fy, fz);
   if (cudaGetLastError() != cudaSuccess) return LBIB_E_CUDA;
   int err = 0;

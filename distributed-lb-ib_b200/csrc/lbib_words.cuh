@@ -132,6 +132,7 @@ struct WordsParams {
   int ngroups;  /* words per x row: nx / V */
   int gpr;      /* threads per row: ngroups (rows packed end to end) */
   int g0, g1;   /* groups whose cells all lie in [4, nx-5] */
+  long pf;      /* L2 prefetch distance in blocks (0: none) */
 };
 
 /* Where a thread's V cells sit and what it does with them. */
@@ -263,6 +264,30 @@ __device__ __forceinline__ void collide2(F2 d[19], F2 drho, F2 dux, F2 duy, F2 d
   lp_pair2<13, 14>(d, uy + uz, i2, drho, rho, t, om, p);
   lp_pair2<15, 16>(d, ux - uy, i2, drho, rho, t, om, p);
   lp_pair2<17, 18>(d, ux + uy, i2, drho, rho, t, om, p);
+}
+
+/* Ask L2 for the words block blk of the flattened (bulk row, word) space
+ * will load: per plane and row, the cells its threads cover plus one on
+ * either side (the odd step's x shifts). */
+template <typename T, int V, int PAR>
+__device__ __forceinline__ void words_prefetch(const WordsParams<T>& b, long blk) {
+  const long t0 = blk * WTPB, t1 = t0 + WTPB - 1;
+  const long r0 = t0 / b.gpr;
+  if (r0 >= b.nrows) return;
+  const long r1 = t1 / b.gpr < b.nrows ? t1 / b.gpr : b.nrows - 1;
+  const int nr = (int)(r1 - r0 + 1);
+  const FluidParamsT<T>& p = b.p;
+  const long N = p.N, sy = p.nx, sz = (long)p.nx * p.ny;
+  for (int i = threadIdx.x; i < 19 * nr; i += WTPB) {
+    const int q = i % 19;
+    const long r = r0 + i / 19;
+    const int y = 3 + (int)(r % b.nry), z = 3 + (int)(r / b.nry);
+    const long gs = r == r0 ? t0 - r0 * b.gpr : 0;
+    const long ge = r == r1 ? t1 - r1 * b.gpr : b.gpr - 1;
+    const long row = ((long)z * p.ny + y) * p.nx;
+    const T* src = PAR ? p.f + opp(q) * N + row - cy(q) * sy - cz(q) * sz : p.f + q * N + row;
+    l2_prefetch(src + gs * V - 1, src + (ge + 1) * V + 1, p.f, p.f + 19 * N);
+  }
 }
 
 /* Collide the V cells and store them (AA pushes assembled across lanes). */
@@ -446,6 +471,7 @@ __host__ __forceinline__ void words_geometry(WordsParams<T>& b, int V, int nx, i
   b.gpr = b.ngroups;
   b.g0 = (4 + V - 1) / V;
   b.g1 = (nx - 4) / V - 1;
+  b.pf = 0;
 }
 
 }  // namespace lbib

@@ -42,24 +42,40 @@ class RunState:
     mass: float
     sheets0: List[np.ndarray] = field(default_factory=list)
     sheets: List[np.ndarray] = field(default_factory=list)
+    stages_ms: Dict[str, float] = field(default_factory=dict)   # per step, over the profiled steps
+    variant: int = -1                                            # autotuned word-kernel variant
 
 
-def run_case(case, steps: int, precision: str, chunk: int = 500) -> RunState:
-    """Advance `case` for `steps` steps in `precision`; device-timed seconds."""
+def run_case(case, steps: int, precision: str, chunk: int = 500, autotune: bool = False,
+             profile_steps: int = 0) -> RunState:
+    """Advance `case` for `steps` steps in `precision`; device-timed seconds.
+    With `autotune` the fastest fluid-kernel variant is chosen first (the run
+    itself is unchanged by it); the last `profile_steps` steps are also timed
+    per stage (CUDA events between the stages)."""
     import torch
 
     s = lbib.Solver(case, precision=precision)
     try:
+        variant = -1
+        if autotune and s.variants() > 1:
+            variant, _ = s.autotune(8)
         sheets0 = [s.sheet(k) for k in range(len(case.sheets))]
         mass0 = float(s.conservation()[0])
         stream = torch.cuda.ExternalStream(s.stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        left = steps
+        prof = min(max(profile_steps, 0), steps)
+        left = steps - prof
         while left > 0:
             n = min(chunk, left)
             s.run(n)
             left -= n
+        stages = {}
+        if prof:
+            s.profile_begin()
+            s.run(prof)
+            st, n = s.profile_end()
+            stages = {k: v / max(n, 1) for k, v in st.items()}
         e1.record(stream)
         e1.synchronize()
         rho, ux, uy, uz = s.moments()
@@ -67,7 +83,7 @@ def run_case(case, steps: int, precision: str, chunk: int = 500) -> RunState:
         return RunState(precision, steps, e0.elapsed_time(e1) / 1e3,
                         np.stack([ux[sl], uy[sl], uz[sl]]), rho[sl].copy(), mass0,
                         float(s.conservation()[0]), sheets0,
-                        [s.sheet(k) for k in range(len(case.sheets))])
+                        [s.sheet(k) for k in range(len(case.sheets))], stages, variant)
     finally:
         s.close()
 

@@ -83,6 +83,9 @@ def run_sweep(problems, steps: int, precision: str = "f16-flow", autotune: bool 
         gpu_s = e0.elapsed_time(e1) / 1e3
         codes, failed_at = b.status()
         tips = [tip_displacement(sheets0[k], b.sheet(k)) for k in range(len(b))]
+        # lattice-site steps advanced: a stopped problem's sites up to its stop step
+        ran = np.where(codes != 0, np.minimum(failed_at, steps), steps)
+        site_steps = int(sum(p.nx * p.ny * p.nz * int(n) for p, n in zip(problems, ran)))
         cells = b.cells
         launches = b.kernel_launches - l0
     finally:
@@ -91,7 +94,7 @@ def run_sweep(problems, steps: int, precision: str = "f16-flow", autotune: bool 
             "points_per_s": len(problems) / wall, "wall_s": wall, "gpu_s": gpu_s, "setup_s": t_setup,
             "mlups": cells * steps / gpu_s / 1e6, "cells": cells, "kernel_launches": launches,
             "stopped": int((codes != 0).sum()), "stopped_at": [int(s) for s in failed_at[codes != 0]],
-            "completed": [bool(c == 0) for c in codes],
+            "completed": [bool(c == 0) for c in codes], "site_steps": site_steps,
             "tip_displacement": tips, "autotune": tuned}
 
 

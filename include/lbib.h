@@ -433,10 +433,14 @@ int lbib_stage(GV gv, int which);
  * Its scratch (per 32-node chunk the stencil bounding box, the box of all
  * stencils and an error word) is one file-scope device array of ~192 KiB,
  * which every GPU that loads the library keeps until the process exits.
- * The first call on each device looks up that array's device address with
- * the device current; make that first call before any stream capture.  All
- * calls share the array: calls whose work overlaps on the GPU (other
- * streams, other host threads on the same device) race -- serialise them. */
+ * Every call looks up that array's device address in the current device's
+ * context (the first call on a device loads the library's module there).
+ * The call reads its error word back with a copy and synchronises `stream`
+ * before it returns, so it must not be called while `stream` is being
+ * captured into a CUDA graph.  It returns LBIB_E_CUDA without doing any work
+ * if a CUDA launch error from earlier work is pending.  All calls share the
+ * array: calls whose work overlaps on the GPU (other streams, other host
+ * threads on the same device) race -- serialise them. */
 #define LBIB_NOALLOC_MAX_NODES (1 << 18)
 int lbib_spread_force_noalloc(const double* nodes, long num_nodes, int nx, int ny, int nz,
                               double* fx, double* fy, double* fz, void* stream);

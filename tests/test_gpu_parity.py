@@ -148,6 +148,21 @@ def test_stencil_leaving_grid_is_an_error(gpu):
     s.close()
 
 
+@pytest.mark.parametrize("bad", [float("nan"), 1e300, float("-inf")])
+def test_nonfinite_node_is_a_stencil_error(gpu, bad):
+    """A NaN or huge coordinate fails the grid check (on the double itself),
+    as the reference's "out of bound" exit does, instead of being converted
+    to an in-range int stencil start."""
+    case, _ = SMALL_CASES["base"]
+    s = lbib.Solver(case)
+    sh = s.sheet().copy()
+    sh[2, 3, 1] = bad
+    s.set_sheet(0, sh)
+    with pytest.raises(lbib.LbibError, match="stencil"):
+        s.run(2)
+    s.close()
+
+
 @pytest.mark.slow
 def test_c0_1000_steps(gpu):
     """The reference's own workload (128x64x64, 52x52 sheet) for 1000 steps:

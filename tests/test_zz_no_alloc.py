@@ -31,13 +31,18 @@ def _entry():
     return f
 
 
-def _call(fn, nodes, case, dev):
+def _call(fn, nodes, case, dev, stream=None):
+    """One call on `stream` (a torch.cuda.Stream, or None: the legacy default
+    stream); the buffers are made on that stream so the call sees them."""
     n = case.nx * case.ny * case.nz
-    d_nodes = torch.from_numpy(np.ascontiguousarray(nodes)).to(dev)
-    out = torch.full((3, n), float("nan"), dtype=torch.float64, device=dev)
-    rc = fn(d_nodes.data_ptr(), nodes.shape[0], case.nx, case.ny, case.nz,
-            out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), None)
-    return rc, out.cpu().numpy().reshape(3, case.nz, case.ny, case.nx)
+    with torch.cuda.stream(stream if stream is not None else torch.cuda.default_stream(dev)):
+        d_nodes = torch.from_numpy(np.ascontiguousarray(nodes)).to(dev)
+        out = torch.full((3, n), float("nan"), dtype=torch.float64, device=dev)
+        rc = fn(d_nodes.data_ptr(), nodes.shape[0], case.nx, case.ny, case.nz,
+                out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(),
+                None if stream is None else stream.cuda_stream)
+        got = out.cpu().numpy().reshape(3, case.nz, case.ny, case.nx)
+    return rc, got
 
 
 def test_noalloc_spread_equals_gv_spread_twice(gpu):
@@ -46,6 +51,7 @@ def test_noalloc_spread_equals_gv_spread_twice(gpu):
     dev = torch.device("cuda", 0)
     fn = _entry()
     s = lbib.Solver(case)
+    side = torch.cuda.Stream(dev)
     for call, steps in enumerate([3, 4]):
         s.run(steps)
         # the GV path's spread of the current sheet (start of the next step)
@@ -58,6 +64,11 @@ def test_noalloc_spread_equals_gv_spread_twice(gpu):
         for a, b in zip(got, ref):
             np.testing.assert_array_equal(a, b)
         assert np.count_nonzero(got[0]) > 0
+        # the same on a caller's own (non-default) stream
+        rc, got = _call(fn, nodes, case, dev, stream=side)
+        assert rc == 0, f"call {call} on a side stream: {rc}"
+        for a, b in zip(got, ref):
+            np.testing.assert_array_equal(a, b)
         # finish the step the stages began
         for st in ["collide", "moments", "move"]:
             s.stage(st)
@@ -83,3 +94,14 @@ def test_noalloc_limits_and_errors(gpu):
     rc, got = _call(fn, bad, case, dev)
     assert rc == E_STENCIL
     assert not np.any(got)
+    # NaN and huge coordinates are outside the grid too (tested on the double,
+    # not after an int conversion that would map NaN to 0)
+    for v in (float("nan"), 1e300, -1e300, float("inf")):
+        bad = nodes.copy()
+        bad[5, 1] = v
+        rc, got = _call(fn, bad, case, dev)
+        assert rc == E_STENCIL, v
+        assert not np.any(got), v
+    # the regular entry point's result is back after an error
+    rc, got = _call(fn, nodes, case, dev)
+    assert rc == 0 and np.count_nonzero(got[0]) == 0   # zero elastic force: zero spread
