@@ -458,6 +458,9 @@ def run_lbib(args):
     c2_leg = None
     if args.c2_steps > 0 and args.precision == "f64":
         c2_leg = run_c2_leg(args, group, peak)
+    sur_leg = None
+    if args.sur_train > 0 and args.precision == "f64" and world == 1:
+        sur_leg = run_surrogate_leg(args)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -471,7 +474,8 @@ def run_lbib(args):
                              "bytes_per_launch": bytes_launch, "launch_ms": fluid_ms},
                 "stages_ms_per_step": {k: v / max(nprof, 1) for k, v in stage_ms.items()},
                 "gpu_launches": launches, "autotune": tuned, "fp16_store": lp,
-                "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "sweep": sweep_leg, "c2": c2_leg}
+                "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "sweep": sweep_leg, "c2": c2_leg,
+                "surrogate": sur_leg}
         print(json.dumps(line), flush=True)
     group.close()
     return 0
@@ -571,6 +575,43 @@ def run_c2_leg(args, group, peak):
     return out
 
 
+def run_surrogate_leg(args):
+    """The learned sweep (surrogate.py): training runs of the batched solver
+    (96 x 48 x 48, 32 x 32 free sheet, T = 3000, default_rng(2)), the MLP
+    trained by the library's own tcgen05 kernels, re-run thresholds
+    calibrated on a quarter of the training runs, then held-out sweep points
+    (default_rng(3)) screened -- reported by the surrogate or re-run by the
+    batched solver in FP16 storage -- against the plain FP64 batched sweep
+    of the same points, which also judges every point (tip displacement of
+    the last fiber row within 2%, or 0.02 lattice units).  Sizes are cut
+    from the workload's 4096 / 2048 so that the leg stays near two minutes;
+    the line states them."""
+    import surrogate
+    t0 = time.perf_counter()
+    r = surrogate.pipeline(train_n=args.sur_train, eval_n=args.sur_eval, steps=3000, every=100,
+                           iters=args.sur_iters, members=3, calib_frac=0.25, target=0.99)
+    e = r["evaluation"]
+    return {"workload": f"learned sweep, 96x48x48 lattice, 32x32 sheet, T=3000: {args.sur_train} training runs "
+                        f"(cut from 4096), {args.sur_eval} held-out points (cut from 2048), MLP 5->4x256->192 x3 "
+                        f"members, {args.sur_iters} Adam steps of 1024",
+            "unit": "points/s",
+            "plain_fp64_points_per_s": e["plain_points_per_s"], "plain_fp64_s": e["plain_fp64_s"],
+            "surrogate_points_per_s": e["surrogate_points_per_s"], "surrogate_s": e["surrogate_s"],
+            "speedup_vs_plain_fp64": e["speedup"],
+            "reported_by_surrogate": e["reported_by_surrogate"], "rerun": e["rerun"], "rerun_why": e["rerun_why"],
+            "rerun_precision": e["rerun_precision"],
+            "right_frac": e["right_frac"],
+            "right_points_per_s": e["right"] / e["surrogate_s"],
+            "reported_completed": e["reported_completed"],
+            "reported_completed_tip_within_2pct": e["reported_completed_tip_within_2pct"],
+            "completed": e["completed"], "completed_tip_within_2pct": e["completed_tip_within_2pct"],
+            "stop_prediction_accuracy": e["stop_prediction_accuracy"],
+            "training_runs_s": r["training_runs"]["seconds"], "training_s": r["training"]["seconds"],
+            "calibration": r["calibration"], "leg_wall_s": time.perf_counter() - t0,
+            "criterion": "a point is right when its stop/complete outcome matches the FP64 run and, if it "
+                         "completes, its tip displacement is within 2% (or 0.02 lattice units) of the FP64 run's"}
+
+
 def run_lp_form(args, case, ref_solver, group, value64, peak):
     """Time the low-precision storage form (default f16-flow: FP16 deviations
     from the inflow equilibrium, FP32 arithmetic) on the same workload and
@@ -634,6 +675,10 @@ def main():
     ap.add_argument("--sweep-steps", type=int, default=2000)
     ap.add_argument("--c2-steps", type=int, default=2000,
                     help="steps of the 512^3 precision leg (FP64 vs FP16 storage; 0: skip)")
+    ap.add_argument("--sur-train", type=int, default=2048,
+                    help="training runs of the learned-sweep leg (0: skip; one GPU only)")
+    ap.add_argument("--sur-eval", type=int, default=512, help="held-out points of the learned-sweep leg")
+    ap.add_argument("--sur-iters", type=int, default=8000, help="Adam steps per surrogate member")
     ap.add_argument("--lp-form", default="f16-flow",
                     help="low-precision form timed beside the FP64 leg (or 'none')")
     ap.add_argument("--variant", type=int, default=None,

@@ -84,8 +84,8 @@ __global__ void __launch_bounds__(WTPB, MINB) lbib_b_words(const WordsParams<T>*
   block_copy(sb, WP + m.x);
   const long first = (long)m.y * WTPB;
   words_item<T, V, PAR>(sb, first + threadIdx.x);
-  const long r0 = (first + sb.gpr - 1) / sb.gpr;
-  long r1 = (first + WTPB + sb.gpr - 1) / sb.gpr;
+  const long r0 = fdiv((unsigned)(first + sb.gpr - 1), sb.dgpr);
+  long r1 = fdiv((unsigned)(first + WTPB + sb.gpr - 1), sb.dgpr);
   if (r1 > sb.nrows) r1 = sb.nrows;
   for (long i = threadIdx.x; i < 4 * (r1 - r0); i += WTPB) edge_cell<T, PAR>(sb.p, sb.nry, (int)(r0 + i / 4), (int)(i & 3));
 }

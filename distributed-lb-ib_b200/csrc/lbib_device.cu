@@ -87,7 +87,8 @@ static void derive_boundaries(lbib_device* d) {
   /* the y walls skip z rows ncx*cs-2, ncx*cs-1 when num_cubes_x < num_cubes_z
      (lbm_ib.c:2378, 2414) */
   d->yskip_z0 = -1;
-  if ((d->compat & 2) && d->ncx < d->ncz) d->yskip_z0 = d->ncx * d->cube_size - 2;
+  if ((d->compat & 2) && d->ncx < d->ncz && !(d->compat & LBIB_OPT_PERIODIC_Z))
+    d->yskip_z0 = d->ncx * d->cube_size - 2;
 }
 
 extern "C" int lbdev_bulk_rows(const lbib_device* d, int* nrows_y, int* nrows_z);

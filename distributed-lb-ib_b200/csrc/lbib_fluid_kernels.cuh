@@ -101,6 +101,10 @@ struct Form<T, false> {
   static __device__ __forceinline__ void initial(const P& p, Mom<R>& m) {
     m.rho = p.rho0; m.ux = p.ux0; m.uy = 0.0; m.uz = 0.0;
   }
+  /* the first step's moments of a cell x in [3, nx-4] */
+  static __device__ __forceinline__ void initial_bulk(const P& p, Mom<R>& m) {
+    m.rho = p.rho0; m.ux = p.ux_rest; m.uy = 0.0; m.uz = 0.0;
+  }
   static __device__ __forceinline__ void from_tile(const P&, const double* U, int cell, Mom<R>& m) {
     m.rho = U[cell]; m.ux = U[64 + cell]; m.uy = U[128 + cell]; m.uz = U[192 + cell];
   }
@@ -130,6 +134,9 @@ struct Form<T, true> {
   using P = FluidParamsT<T>;
   static __device__ __forceinline__ void initial(const P& p, Mom<R>& m) {
     m.rho = (float)(p.rho0 - p.rhos); m.ux = (float)(p.ux0 - p.uxs); m.uy = 0.0f; m.uz = 0.0f;
+  }
+  static __device__ __forceinline__ void initial_bulk(const P& p, Mom<R>& m) {
+    m.rho = (float)(p.rho0 - p.rhos); m.ux = (float)(p.ux_rest - p.uxs); m.uy = 0.0f; m.uz = 0.0f;
   }
   static __device__ __forceinline__ void from_tile(const P& p, const double* U, int cell, Mom<R>& m) {
     m.rho = (float)(U[cell] - p.rhos); m.ux = (float)(U[64 + cell] - p.uxs);
@@ -207,8 +214,10 @@ __device__ __forceinline__ void step_cell(const FluidParamsT<T>& p, int x, int y
   const int cell = cell_in_tile(x, y, z);
   using F = Form<T>;
   Mom<R> m;
-  if (kind >= K_SEMI || p.first) {
+  if (kind >= K_SEMI) {
     F::initial(p, m);
+  } else if (p.first) {
+    F::initial_bulk(p, m);
   } else {
     const int sp = p.slot_prev[tile];
     if (sp >= 0) F::from_tile(p, p.Uprev + (long)sp * 256, cell, m);
@@ -246,7 +255,7 @@ __device__ __forceinline__ bool tile_moment_values(const FluidParamsT<T>& p, int
   const int tx = tile % p.ntx, ty = (tile / p.ntx) % p.nty, tz = tile / (p.ntx * p.nty);
   if (tx * 4 < p.olo || tx * 4 >= p.ohi) return false;
   const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
-  rho = p.rho0; ux = p.ux0; uy = 0.0; uz = 0.0;
+  rho = p.rho0; ux = (x >= 3 && x <= p.nx - 4) ? p.ux_rest : p.ux0; uy = 0.0; uz = 0.0;
   if (x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
     const long idx = sidx(p, x, y, z);
     R f[19];
@@ -292,7 +301,7 @@ __global__ void lbib_field_moments(FluidParamsT<T> p, int have_step, double* __r
   const int y = blockIdx.y, z = blockIdx.z;
   if (x >= p.ohi) return;
   const long idx = sidx(p, x, y, z);
-  double rho = p.rho0, ux = p.ux0, uy = 0.0, uz = 0.0;
+  double rho = p.rho0, ux = (x >= 3 && x <= p.nx - 4) ? p.ux_rest : p.ux0, uy = 0.0, uz = 0.0;
   if (have_step && x >= 3 && x <= p.nx - 4 && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) {
     R f[19];
     load_pre<PAR>(p, x, y, z, idx, classify(p, x, y, z), f);
@@ -380,13 +389,16 @@ static __global__ void __launch_bounds__(256) lbib_sum_rows(const double* __rest
   if (threadIdx.x < 4) out[threadIdx.x] = sh[threadIdx.x][0];
 }
 
-/* init_df1 (lbm_ib.c:2725-2767): every cell in natural order. */
+/* init_df1 (lbm_ib.c:2725-2767): every cell in natural order; from rest
+ * (an option) the cells x in [3, nx-4] start at u = 0. */
 template <typename T>
 __global__ void lbib_init_pop(FluidParamsT<T> p, T* __restrict__ f, long count) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
+  const int x = (int)(i % p.sx) + p.gx0;
+  const double ux = (x >= 3 && x <= p.nx - 4) ? p.ux_rest : p.ux0;
 #pragma unroll
-  for (int q = 0; q < 19; ++q) f[q * count + i] = Pop<T>::put(Form<T>::stored_initial(q, p.rho0, p.ux0, p));
+  for (int q = 0; q < 19; ++q) f[q * count + i] = Pop<T>::put(Form<T>::stored_initial(q, p.rho0, ux, p));
 }
 
 /* init_df_inout (lbm_ib.c:1610-1670): the fixed inlet/outlet planes. */
@@ -408,7 +420,9 @@ FluidParamsT<T> make_params_t(lbib_device* d, int first) {
   p.xlo = d->x_lo > 2 ? d->x_lo : 2;
   p.xhi = d->x_hi - 1 < d->nx - 3 ? d->x_hi - 1 : d->nx - 3;
   p.zin_hi = d->zin_hi; p.yskip_z0 = d->yskip_z0; p.first = first;
+  p.periodic_z = (d->compat & LBIB_OPT_PERIODIC_Z) != 0;
   p.rho0 = d->rho_l; p.ux0 = d->u_l;
+  p.ux_rest = (d->compat & LBIB_OPT_REST_START) ? 0.0 : d->u_l;
   p.omtau = d->omtau; p.invtau = d->invtau;
   p.kw0 = d->kw[0]; p.kw1 = d->kw[1]; p.kw2 = d->kw[2];
   p.cs2 = d->cs2; p.cs4 = d->cs4; p.half_dt = d->half_dt; p.g = d->g_l;

@@ -32,10 +32,109 @@ __global__ void __launch_bounds__(WTPB, MINB) lbib_fluid_step_words(WordsParams<
   /* the plane-adjacent cells x in {2, 3, nx-4, nx-3} of the rows whose first
      word this block holds, while their words are in the caches (their slots
      are theirs alone, so the order within the launch does not matter) */
-  const long r0 = (first + b.gpr - 1) / b.gpr;
-  long r1 = (first + WTPB + b.gpr - 1) / b.gpr;
+  const long r0 = fdiv((unsigned)(first + b.gpr - 1), b.dgpr);
+  long r1 = fdiv((unsigned)(first + WTPB + b.gpr - 1), b.dgpr);
   if (r1 > b.nrows) r1 = b.nrows;
   for (long i = threadIdx.x; i < 4 * (r1 - r0); i += WTPB) edge_cell<T, PAR>(b.p, b.nry, (int)(r0 + i / 4), (int)(i & 3));
+}
+
+/* The word step with TMA-staged loads (lbib_words.cuh): a persistent grid
+ * of CTAs, each keeping STAGES items of bulk copies in flight ahead of its
+ * compute.  Errors (a window outside the buffer, an mbarrier wait that ran
+ * out) go to the state's error word as LBIB_E_CUDA. */
+template <typename T, int PAR, int STAGES, int MINB>
+__global__ void __launch_bounds__(WTPB, MINB) lbib_fluid_step_words_tma(WordsParams<T> b, TmaGeom g, int* err) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t full[STAGES];
+  __shared__ int s_bad;
+  const int t = threadIdx.x, lane = t & 31;
+  const int SB = tma_stage_bytes(g);
+  if (t == 0) {
+    for (int s = 0; s < STAGES; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(cta_smem(&full[s])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_bad = 0;
+  }
+  __syncthreads();
+  if (t == 0)
+    for (int s = 0; s < STAGES; ++s) {
+      const long it = blockIdx.x + (long)s * gridDim.x;
+      if (it < g.nitems) tma_issue<T, PAR>(b, g, it, smem + s * SB, &full[s], &s_bad);
+    }
+  const int k = t / g.segw, w = t - k * g.segw;
+  int j = 0;
+  bool ok = true;
+  for (long it = blockIdx.x; it < g.nitems; it += gridDim.x, ++j) {
+    const int s = j % STAGES;
+    ok = __syncthreads_and(tma_wait(&full[s], (uint32_t)((j / STAGES) & 1)));
+    if (!ok) break;
+    long row0;
+    int w0;
+    tma_item(g, it, row0, w0);
+    /* the thread's word: row row0 + k, word w0 + w */
+    ItemCtx c;
+    const long r = row0 + k;
+    const int gw = w0 + w;
+    const bool inrow = k < g.K && r < b.nrows && gw < g.W;
+    const unsigned rz = fdiv((unsigned)r, b.dnry);
+    c.y = 3 + (int)((unsigned)r - rz * (unsigned)b.nry);
+    c.z = 3 + (int)rz;
+    c.x0 = gw * 4;
+    c.loads = inrow;
+    c.active = inrow && group_here<T, 4>(b, gw, c.y, c.z);
+    c.left_active = __shfl_up_sync(0xffffffffu, c.active, 1);
+    c.right_active = __shfl_down_sync(0xffffffffu, c.active, 1);
+    if (lane == 0) c.left_active = inrow && group_here<T, 4>(b, gw - 1, c.y, c.z);
+    if (lane == 31) c.right_active = inrow && group_here<T, 4>(b, gw + 1, c.y, c.z);
+    c.row = ((long)c.z * b.p.ny + c.y) * b.p.nx;
+    float d[19 * 4];
+    const uint16_t* st = reinterpret_cast<const uint16_t*>(smem + s * SB) + (long)(k < g.K ? k : 0) * g.win;
+    const int e0 = 4 * w + 8;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      Word<T, 4> wd;
+      if (inrow) {
+        const Word<__half, 4> h = smem_word<PAR>(st + (long)q * g.K * g.win, e0, q);
+        wd.r[0] = h.r[0]; wd.r[1] = h.r[1];
+      } else {
+        wd.clear();
+      }
+      wd.unpack(d + q * 4, 1);
+    }
+    words_collide_store<T, 4, PAR>(b.p, c, lane, d);
+    __syncthreads();      /* every thread is done with stage s */
+    if (t == 0) {
+      const long nxt = it + (long)STAGES * gridDim.x;
+      if (nxt < g.nitems) tma_issue<T, PAR>(b, g, nxt, smem + s * SB, &full[s], &s_bad);
+    }
+  }
+  if (!ok) {
+    /* a wait ran out: let the copies already issued land (bounded) before
+       the CTA's shared memory is released */
+    if (t == 0)
+      for (int i = 0; i < STAGES; ++i) {
+        const int s = (j + i) % STAGES;
+        const long it = blockIdx.x + (long)(j + i) * gridDim.x;
+        if (it < g.nitems) tma_wait(&full[s], (uint32_t)(((j + i) / STAGES) & 1));
+      }
+    __syncthreads();
+  }
+  /* the plane-adjacent cells x in {2, 3, nx-4, nx-3} of the rows whose
+     items start at word 0, after the staged loop so that their global
+     loads do not stall it: 4 K cells per such item, all threads at once */
+  if (ok) {
+    const long per = 4L * g.K;
+    const long nmine = g.nitems > blockIdx.x ? (g.nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    for (long e = t; e < nmine * per; e += WTPB) {
+      const long it = blockIdx.x + (e / per) * gridDim.x;
+      long row0;
+      int w0;
+      tma_item(g, it, row0, w0);
+      const long r = row0 + (e % per) / 4;
+      if (w0 == 0 && r < b.nrows) edge_cell<T, PAR>(b.p, b.nry, (int)r, (int)(e & 3));
+    }
+  }
+  if (t == 0 && (!ok || s_bad)) atomicCAS(err, 0, -2);   /* LBIB_E_CUDA */
 }
 
 /* Cells of this step's forced tiles inside the word kernel's range; a
@@ -67,6 +166,7 @@ int launch_words(lbib_device* d, const FluidParamsT<T>& p) {
   words_geometry(b, V, d->nx, nry, nrz);
   b.pf = (long)d->l2_pf * sm_count() * MINB;
   const long threads = b.nrows * b.gpr;
+  if (threads + WTPB >= (1L << 31)) return -1;   /* item_ctx divides 32-bit indices */
   const unsigned blocks = (unsigned)((threads + WTPB - 1) / WTPB);
   const int zb = 2 + nrz, c = d->cur;
   const unsigned fblocks = (unsigned)sm_count() * 8;
@@ -81,13 +181,59 @@ int launch_words(lbib_device* d, const FluidParamsT<T>& p) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+/* The TMA-staged word step (16-bit storage) and the forced cells; the
+ * plain word kernel where the row geometry does not suit it. */
+template <typename T, int STAGES, int MINB>
+int launch_words_tma(lbib_device* d, const FluidParamsT<T>& p) {
+  WordsParams<T> b;
+  b.p = p;
+  int nry = 0, nrz = 0;
+  if (!lbdev_bulk_rows(d, &nry, &nrz)) return 0;
+  words_geometry(b, 4, d->nx, nry, nrz);
+  TmaGeom g;
+  if (!tma_geometry(g, d->nx, b.nrows)) return launch_words<T, 4, MINB>(d, p);
+  const int smem = STAGES * tma_stage_bytes(g);
+  static int attr[2] = {0, 0};
+  if (smem > attr[0]) {
+    if (cudaFuncSetAttribute(lbib_fluid_step_words_tma<T, 0, STAGES, MINB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+        cudaFuncSetAttribute(lbib_fluid_step_words_tma<T, 1, STAGES, MINB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+      return -2;
+    attr[0] = smem;
+  }
+  const long cap = (long)sm_count() * MINB;
+  const unsigned blocks = (unsigned)(g.nitems < cap ? g.nitems : cap);
+  const int zb = 2 + nrz, c = d->cur;
+  const unsigned fblocks = (unsigned)sm_count() * 8;
+  if (d->parity == 0) {
+    lbib_fluid_step_words_tma<T, 0, STAGES, MINB><<<blocks, WTPB, smem, d->stream>>>(b, g, d->err);
+    lbib_forced_cells<T, 0><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
+  } else {
+    lbib_fluid_step_words_tma<T, 1, STAGES, MINB><<<blocks, WTPB, smem, d->stream>>>(b, g, d->err);
+    lbib_forced_cells<T, 1><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
+  }
+  d->kernel_launches += 2;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+/* One-grid variants beyond the word-kernel ones of lbib_words.cuh (16-bit
+ * storage): {stages, resident CTAs per SM} of the TMA-staged kernel. */
+constexpr int kTmaVariants = 3;
+
 template <typename T>
 int lp_step(lbib_device* d) {
   FluidParamsT<T> p = make_params_t<T>(d, d->steps == 0);
   if (launch_step_rows_t<T>(d, p)) return -2;
   if (!d->use_bulk) return 0;
-  return with_variant<T>(d->lp_variant < 0 ? 0 : d->lp_variant,
-                         [&](auto V, auto MINB) { return launch_words<T, V, MINB>(d, p); });
+  const int v = d->lp_variant < 0 ? 0 : d->lp_variant;
+  if constexpr (sizeof(T) == 2) {
+    const int nw = word_variants(d->prec);
+    if (v == nw) return launch_words_tma<T, 2, 4>(d, p);
+    if (v == nw + 1) return launch_words_tma<T, 3, 3>(d, p);
+    if (v == nw + 2) return launch_words_tma<T, 2, 5>(d, p);
+  }
+  return with_variant<T>(v, [&](auto V, auto MINB) { return launch_words<T, V, MINB>(d, p); });
 }
 
 }  // namespace
@@ -148,5 +294,6 @@ extern "C" int lbdev_lp_sums(lbib_device* d, double* part, double* out) {
 
 /* Word-kernel variants available for a precision (1 for FP64). */
 extern "C" int lbdev_lp_variants(int prec) {
-  return LBIB_PREC_TYPE(prec) == LBIB_PREC_F64 ? 1 : word_variants(prec);
+  if (LBIB_PREC_TYPE(prec) == LBIB_PREC_F64) return 1;
+  return word_variants(prec) + (LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? 0 : kTmaVariants);
 }

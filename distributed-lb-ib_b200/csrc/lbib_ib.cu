@@ -61,11 +61,12 @@ __global__ void __launch_bounds__(64) lbib_spread_gather_scan(const double* __re
   }
 }
 
+/* Nodes [i0, i1) of the concatenated sheets. */
 __global__ void lbib_move_nodes(double* __restrict__ nodes, const double* __restrict__ W, const int* __restrict__ st,
-                                long S, int ntx, int nty, const int* __restrict__ slot, const double* __restrict__ Utile,
-                                double dt, const int* err) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= S) return;
+                                long i0, long i1, int ntx, int nty, const int* __restrict__ slot,
+                                const double* __restrict__ Utile, double dt, const int* err) {
+  const long i = i0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1) return;
   if (*(volatile const int*)err) return;
   move_node(nodes, W, st, i, ntx, nty, slot, Utile, dt);
 }
@@ -127,12 +128,25 @@ extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+/* moveFiberSheet over all nodes; with the pinned-row option (no reference
+ * counterpart) row 0 of every sheet is left where it is: one launch per
+ * sheet over its rows 1 .. rows-1. */
 extern "C" int lbdev_launch_move(lbib_device* d) {
   const int c = d->cur;
-  const unsigned nb = (unsigned)((d->S + 127) / 128);
-  lbib_move_nodes<<<nb, 128, 0, d->stream>>>(d->nodes, d->W, d->st, d->S, d->ntx, d->nty, d->tile_slot[c],
-                                             d->Utile[c], (double)d->dt, d->err);
-  d->kernel_launches++;
+  if (!(d->compat & LBIB_OPT_PIN_ROW0)) {
+    const unsigned nb = (unsigned)((d->S + 127) / 128);
+    lbib_move_nodes<<<nb, 128, 0, d->stream>>>(d->nodes, d->W, d->st, 0, d->S, d->ntx, d->nty, d->tile_slot[c],
+                                               d->Utile[c], (double)d->dt, d->err);
+    d->kernel_launches++;
+  } else {
+    for (int k = 0; k < d->nsheets; ++k) {
+      const long i0 = d->sh[k].offset + d->sh[k].cols, i1 = d->sh[k].offset + (long)d->sh[k].rows * d->sh[k].cols;
+      const unsigned nb = (unsigned)((i1 - i0 + 127) / 128);
+      lbib_move_nodes<<<nb, 128, 0, d->stream>>>(d->nodes, d->W, d->st, i0, i1, d->ntx, d->nty, d->tile_slot[c],
+                                                 d->Utile[c], (double)d->dt, d->err);
+      d->kernel_launches++;
+    }
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

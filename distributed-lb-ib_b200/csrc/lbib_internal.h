@@ -42,6 +42,12 @@ extern "C" {
 #endif
 #define LBIB_PREC_TYPE(p) ((p) & 15)
 
+#ifndef LBIB_OPT_PERIODIC_Z
+#define LBIB_OPT_PERIODIC_Z 0x100  /* option bits of the compat word, as in include/lbib.h */
+#define LBIB_OPT_REST_START 0x200
+#define LBIB_OPT_PIN_ROW0   0x400
+#endif
+
 typedef struct lbib_sheet_dev {
   int rows, cols;
   long offset;                   /* first node in the concatenated arrays */

@@ -106,7 +106,9 @@ struct FluidParamsT {
   int olo, ohi;          /* columns this state owns: [olo, ohi) */
   int xlo, xhi;          /* columns of I it collides: [xlo, xhi] */
   int zin_hi, yskip_z0, first;
-  double rho0, ux0;
+  int periodic_z;        /* option: z periodic over I (period nz - 4), walls only at y */
+  double rho0, ux0;      /* moments of the plane cells and the tables (the inflow)     */
+  double ux_rest;        /* initial u_x of the cells x in [3, nx-4]: ux0, 0 from rest  */
   double omtau, invtau, kw0, kw1, kw2, cs2, cs4, half_dt, g;
   const int* slot_cur;   /* F(t) tiles */
   const double* Fcur;
@@ -201,13 +203,17 @@ __device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y,
   const bool yskip = (kind == K_WALL) && p.yskip_z0 >= 0 && (z == p.yskip_z0 || z == p.yskip_z0 + 1);
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
-    const int xs = x - cx(q), ys = y - cy(q), zs = z - cz(q);
+    const int xs = x - cx(q), ys = y - cy(q);
+    int zs = z - cz(q);
+    long wrap = 0;   /* periodic z: the source re-enters I at the other side */
+    if (p.periodic_z && zs < 2) { zs += p.nz - 4; wrap = (long)(p.nz - 4) * sz; }
+    if (p.periodic_z && zs > p.nz - 3) { zs -= p.nz - 4; wrap = -(long)(p.nz - 4) * sz; }
     const bool yin = ys >= 2 && ys <= p.ny - 3;
     const bool zin = zs >= 2 && zs <= p.nz - 3;
     const bool xin = xs >= 2 && xs <= p.nx - 3;
     if (xin && yin && zin) {
       if (PAR == 0) f[q] = Pop<T>::get(F[q * N + idx]);
-      else f[q] = Pop<T>::get(F[opp(q) * N + idx - link_offset(q, sy, sz)]);
+      else f[q] = Pop<T>::get(F[opp(q) * N + idx - link_offset(q, sy, sz) + wrap]);
     } else {
       const bool zero = !p.first && (kind == K_SEMI || (yskip && !yin && zin));
       f[q] = zero ? zero_pop(p, q) : bounced(p, q, Pop<T>::get(F[q * N + idx]));
@@ -234,9 +240,13 @@ __device__ __forceinline__ void store_post(const FluidParamsT<T>& p, int x, int 
   }
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
-    const int xt = x + cx(q), yt = y + cy(q), zt = z + cz(q);
+    const int xt = x + cx(q), yt = y + cy(q);
+    int zt = z + cz(q);
+    long wrap = 0;
+    if (p.periodic_z && zt < 2) { zt += p.nz - 4; wrap = (long)(p.nz - 4) * sz; }
+    if (p.periodic_z && zt > p.nz - 3) { zt -= p.nz - 4; wrap = -(long)(p.nz - 4) * sz; }
     const bool in = xt >= 2 && xt <= p.nx - 3 && yt >= 2 && yt <= p.ny - 3 && zt >= 2 && zt <= p.nz - 3;
-    if (in) F[q * N + idx + link_offset(q, sy, sz)] = Pop<T>::put(f[q]);
+    if (in) F[q * N + idx + link_offset(q, sy, sz) + wrap] = Pop<T>::put(f[q]);
     else F[opp(q) * N + idx] = Pop<T>::put(f[q]);
   }
 }

@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/lbib.h"
+#include "lbib_mlp_tc.cuh"
 
 namespace {
 
@@ -37,6 +38,7 @@ enum Epi {
   EPI_STORE = 0,        /* C (fp32) = acc                                  */
   EPI_BIAS_GELU = 1,    /* Z = acc + b (fp32 out0), A = gelu(Z) (bf16 out1) */
   EPI_BIAS = 2,         /* Y = acc + b (fp32 out0)                          */
+  EPI_GELU_BACK = 3,    /* dZ = acc * gelu'(Z) (bf16 out1), Z in `aux`      */
 };
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
@@ -130,6 +132,139 @@ __global__ void __launch_bounds__(128) mlp_gemm(const __nv_bfloat16* __restrict_
       }
 }
 
+/* The same product and epilogues on the tcgen05 tensor cores (FP32
+ * accumulator in TMEM; lbib_mlp_tc.cuh): a 128 x BN tile per 128-thread
+ * CTA, K in double-buffered slices of 64.  `err` is set if an mbarrier wait
+ * ran out (the tile is then not written).
+ *
+ * Split K (gridDim.z = S > 1, EPI_STORE only): CTA z sums the K slices
+ * [z Kc, (z+1) Kc) and writes its partial tile to ws[z]; the CTA that
+ * finishes a tile last (a per-tile counter) adds the S partials in z order
+ * into out0 and resets the counter -- the same bits whatever the order in
+ * which the CTAs run.  `aux` is the bias, or Z for EPI_GELU_BACK. */
+constexpr int TC_BN = 64;
+constexpr int kMaxSplit = 8;      /* split-K factors 1, 2, 4, 8             */
+constexpr int kMaxTiles = 4096;   /* output tiles a split GEMM may have     */
+constexpr int TC_SMEM = 2 * (lbib_tc::BM + TC_BN) * lbib_tc::BK * 2 + 64;
+
+template <int EPI>
+__global__ void __launch_bounds__(lbib_tc::NT) mlp_gemm_tc(const __nv_bfloat16* __restrict__ A, long am, long ak,
+                                                         const __nv_bfloat16* __restrict__ B, long bk, long bn, int M,
+                                                         int N, int K, float* __restrict__ out0,
+                                                         __nv_bfloat16* __restrict__ out1, long ldc,
+                                                         const float* __restrict__ aux, int* __restrict__ err,
+                                                         float* __restrict__ ws, int* __restrict__ tile_cnt) {
+  const float* bias = aux;
+  using namespace lbib_tc;
+  constexpr int BN = TC_BN;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(smem);             /* [2][BM * BK] */
+  __nv_bfloat16* sB = sA + 2 * BM * BK;                                    /* [2][BN * BK] */
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sB + 2 * BN * BK);           /* [2]          */
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  if (warp == 0) tmem_alloc<BN>(tslot);
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  /* the B operand is staged as X(n, k) = B[n*bn + k*bk] */
+  const int ma = stage_mode(A, am, ak, M, K), mb = stage_mode(B, bn, bk, N, K);
+  const uint32_t idesc = instr_desc_bf16(BM, BN, ma == ST_MN_VEC, mb == ST_MN_VEC);
+  /* this CTA's K slices: all of them, or its share of a split */
+  const int nk_all = (K + BK - 1) / BK;
+  const int S = gridDim.z, per = (nk_all + S - 1) / S;
+  const int kt0 = blockIdx.z * per;
+  const int nk = kt0 + per <= nk_all ? per : (nk_all > kt0 ? nk_all - kt0 : 0);
+  bool ok = true;
+  for (int kk = 0; kk < nk; ++kk) {
+    const int kt = kt0 + kk;
+    const int b = kk & 1;
+    if (kk >= 2 && !__syncthreads_and(mbar_wait(&bar[b], ((kk - 2) >> 1) & 1))) {
+      ok = false;
+      break;
+    }
+    __nv_bfloat16* a_s = sA + b * BM * BK;
+    __nv_bfloat16* b_s = sB + b * BN * BK;
+    stage_operand<BM>(a_s, A, am, ak, m0, M, kt * BK, K, ma);
+    stage_operand<BN>(b_s, B, bn, bk, n0, N, kt * BK, K, mb);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int s = 0; s < BK / 16; ++s) {
+        const uint64_t da = smem_desc(smem_u32(a_s) + s * 2 * (BM / 8) * 128, (BM / 8) * 128, 128);
+        const uint64_t db = smem_desc(smem_u32(b_s) + s * 2 * (BN / 8) * 128, (BN / 8) * 128, 128);
+        mma_bf16(tmem, da, db, idesc, (kk > 0 || s > 0) ? 1u : 0u);
+      }
+      mma_commit(&bar[b]);
+    }
+  }
+  /* the last commit covers every MMA of the tile */
+  if (nk > 0) ok = __syncthreads_and(ok && mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1));
+  tc_fence_after();
+  __shared__ int s_last;
+  if (ok) {
+    const int m = m0 + warp * 32 + lane;
+    float* part = S > 1 ? ws + (long)blockIdx.z * M * ldc : nullptr;
+    for (int c = 0; c < BN; c += 16) {
+      float v[16];
+      if (nk > 0) tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      else for (int i = 0; i < 16; ++i) v[i] = 0.0f;   /* no K slice in this split */
+      if (m >= M) continue;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int n = n0 + c + i;
+        if (n >= N) continue;
+        float x = v[i];
+        if (EPI == EPI_STORE) {
+          if (S > 1) part[(long)m * ldc + n] = x;
+          else out0[(long)m * ldc + n] = x;
+        } else if (EPI == EPI_GELU_BACK) {
+          out1[(long)m * ldc + n] = __float2bfloat16(x * gelu_grad(aux[(long)m * ldc + n]));
+        } else {
+          x += bias[n];
+          out0[(long)m * ldc + n] = x;
+          if (EPI == EPI_BIAS_GELU) out1[(long)m * ldc + n] = __float2bfloat16(gelu(x));
+        }
+      }
+    }
+    if (EPI == EPI_STORE && S > 1) {
+      /* the last CTA of this tile adds the partials in split order */
+      __threadfence();
+      __syncthreads();
+      if (t == 0) {
+        const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+        s_last = atomicAdd(&tile_cnt[tile], 1) == S - 1;
+        if (s_last) tile_cnt[tile] = 0;
+      }
+      __syncthreads();
+      if (s_last) {
+        __threadfence();
+        for (int e = t; e < BM * BN; e += NT) {
+          const int mm = m0 + e / BN, nn = n0 + e % BN;
+          if (mm >= M || nn >= N) continue;
+          float acc = 0.0f;
+          for (int z = 0; z < S; ++z) acc += ws[(long)z * M * ldc + (long)mm * ldc + nn];
+          out0[(long)mm * ldc + nn] = acc;
+        }
+      }
+    }
+  } else if (t == 0) {
+    atomicExch(err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free<BN>(tmem);
+}
+
 /* X (fp32, [B][w_in]) -> bf16 [B][w_pad], pad columns 0. */
 __global__ void mlp_input(const float* __restrict__ X, int B, int w, int wp, __nv_bfloat16* __restrict__ out) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -184,13 +319,24 @@ __global__ void mlp_gelu_back(const float* __restrict__ dA, const float* __restr
   if (i < n) dZ[i] = __float2bfloat16(dA[i] * gelu_grad(Z[i]));
 }
 
-/* db[n] = sum over the batch of dZ[:, n], in a fixed order. */
-__global__ void mlp_bias_grad(const __nv_bfloat16* __restrict__ dZ, int B, int w, float* __restrict__ db) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= w) return;
+/* db[n] = sum over the batch of dZ[:, n], in a fixed order: thread
+ * (c, g) of a 32 x 32 block sums rows g, g + 32, ... of column 32 blockIdx.x
+ * + c, then the 32 partial sums of a column are added in g order. */
+__global__ void __launch_bounds__(1024) mlp_bias_grad(const __nv_bfloat16* __restrict__ dZ, int B, int w,
+                                                     float* __restrict__ db) {
+  __shared__ float part[32][33];
+  const int c = threadIdx.x, g = threadIdx.y;
+  const int n = blockIdx.x * 32 + c;
   float s = 0.0f;
-  for (int r = 0; r < B; ++r) s += __bfloat162float(dZ[(long)r * w + n]);
-  db[n] = s;
+  if (n < w)
+    for (int r = g; r < B; r += 32) s += __bfloat162float(dZ[(long)r * w + n]);
+  part[g][c] = s;
+  __syncthreads();
+  if (g == 0 && n < w) {
+    float t = 0.0f;
+    for (int k = 0; k < 32; ++k) t += part[k][c];
+    db[n] = t;
+  }
 }
 
 /* Adam on the fp32 master copy; refresh the bf16 weights. */
@@ -229,10 +375,16 @@ struct lbib_mlp {
   long* wbo;            /* [L] offset of W_l in wbf */
   __nv_bfloat16** act;  /* [L+1] bf16 activations [B][wp_l] (act[0] = input) */
   float** z;            /* [L] pre-activations fp32 [B][wp_{l+1}] */
-  float* dA;            /* fp32 [B][max wp] */
-  __nv_bfloat16* dZ;    /* bf16 [B][max wp] */
+  float* dA;            /* fp32 [B][max wp] (the mma.sync path)         */
+  __nv_bfloat16* dZ;    /* bf16 [2][B][max wp]: layer l's dZ, and l-1's  */
+  float* ws;            /* split-K partial tiles                          */
+  long ws_elems;
+  int* tile_cnt;        /* split-K arrivals per output tile (kMaxTiles)   */
   float* part;
   float* d_loss;
+  int* d_err;           /* a tensor-core GEMM's mbarrier wait ran out     */
+  int legacy;           /* LBIB_MLP_LEGACY=1: the warp-level mma.sync GEMM */
+  int maxw;             /* largest padded width                           */
   long steps;
   cudaStream_t stream;  /* where the work runs: own_stream or the caller's */
   cudaStream_t own_stream;
@@ -242,6 +394,46 @@ namespace {
 
 int launch_gemm(lbib_mlp* n, int epi, const __nv_bfloat16* A, long am, long ak, const __nv_bfloat16* B, long bk,
                 long bn, int M, int N, int K, float* out0, __nv_bfloat16* out1, long ldc, const float* bias) {
+  if (!n->legacy) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(mlp_gemm_tc<EPI_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+      cudaFuncSetAttribute(mlp_gemm_tc<EPI_BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+      cudaFuncSetAttribute(mlp_gemm_tc<EPI_BIAS_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+      cudaFuncSetAttribute(mlp_gemm_tc<EPI_GELU_BACK>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+      attr = true;
+    }
+    dim3 grid((unsigned)((N + TC_BN - 1) / TC_BN), (unsigned)((M + lbib_tc::BM - 1) / lbib_tc::BM), 1);
+    /* a long K over few tiles (the weight gradients, K = batch) is split so
+       that ~32 CTAs share it; the split depends on the shape only */
+    if (epi == EPI_STORE) {
+      const int tiles = (int)(grid.x * grid.y), nkt = (K + lbib_tc::BK - 1) / lbib_tc::BK;
+      int sk = 1;
+      while (sk * 2 <= kMaxSplit && tiles * sk < 32 && nkt >= 4 * sk * 2) sk *= 2;
+      if ((long)sk * M * ldc > n->ws_elems || tiles > kMaxTiles) sk = 1;
+      grid.z = (unsigned)sk;
+    }
+    switch (epi) {
+      case EPI_BIAS_GELU:
+        mlp_gemm_tc<EPI_BIAS_GELU><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0,
+                                                                              out1, ldc, bias, n->d_err, n->ws,
+                                                                              n->tile_cnt);
+        break;
+      case EPI_BIAS:
+        mlp_gemm_tc<EPI_BIAS><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1,
+                                                                         ldc, bias, n->d_err, n->ws, n->tile_cnt);
+        break;
+      case EPI_GELU_BACK:
+        mlp_gemm_tc<EPI_GELU_BACK><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0,
+                                                                              out1, ldc, bias, n->d_err, n->ws,
+                                                                              n->tile_cnt);
+        break;
+      default:
+        mlp_gemm_tc<EPI_STORE><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1,
+                                                                          ldc, bias, n->d_err, n->ws, n->tile_cnt);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+  }
   dim3 grid((unsigned)((N + TN - 1) / TN), (unsigned)((M + TM - 1) / TM));
   switch (epi) {
     case EPI_BIAS_GELU:
@@ -275,20 +467,27 @@ int backward(lbib_mlp* n, const float* T, int batch) {
   const int L = n->L;
   const long ny = (long)batch * n->wp[L];
   const unsigned nb = (unsigned)((ny + 255) / 256);
+  const long zst = (long)n->max_batch * n->maxw;       /* the two dZ buffers */
   mlp_mse<<<nb, 256, 0, n->stream>>>(n->z[L - 1], T, batch, n->w[L], n->wp[L], n->dZ, n->part);
   mlp_sum<<<1, 256, 0, n->stream>>>(n->part, (int)nb, 1.0f / ((float)batch * (float)n->w[L]), n->d_loss);
   for (int l = L - 1; l >= 0; --l) {
     const int in = n->wp[l], out = n->wp[l + 1];
+    __nv_bfloat16* dZ = n->dZ + ((L - 1 - l) & 1) * zst;
+    __nv_bfloat16* dZ_prev = n->dZ + ((L - l) & 1) * zst;
     /* dW = dZ^T X: M = out, N = in, K = batch */
-    if (launch_gemm(n, EPI_STORE, n->dZ, 1, out, n->act[l], in, 1, out, in, batch, n->g + n->woff[l], NULL, in, NULL))
+    if (launch_gemm(n, EPI_STORE, dZ, 1, out, n->act[l], in, 1, out, in, batch, n->g + n->woff[l], NULL, in, NULL))
       return -2;
-    mlp_bias_grad<<<(out + 127) / 128, 128, 0, n->stream>>>(n->dZ, batch, out, n->g + n->boff[l]);
+    mlp_bias_grad<<<(out + 31) / 32, dim3(32, 32), 0, n->stream>>>(dZ, batch, out, n->g + n->boff[l]);
     if (l == 0) break;
-    /* dA = dZ W: M = batch, N = in, K = out; then through the GELU of layer l-1 */
+    /* dZ_{l-1} = (dZ W) * gelu'(Z_{l-1}): M = batch, N = in, K = out */
     const __nv_bfloat16* W = n->wbf + n->wbo[l];
-    if (launch_gemm(n, EPI_STORE, n->dZ, out, 1, W, in, 1, batch, in, out, n->dA, NULL, in, NULL)) return -2;
-    const long na = (long)batch * in;
-    mlp_gelu_back<<<(unsigned)((na + 255) / 256), 256, 0, n->stream>>>(n->dA, n->z[l - 1], na, n->dZ);
+    if (n->legacy) {
+      if (launch_gemm(n, EPI_STORE, dZ, out, 1, W, in, 1, batch, in, out, n->dA, NULL, in, NULL)) return -2;
+      const long na = (long)batch * in;
+      mlp_gelu_back<<<(unsigned)((na + 255) / 256), 256, 0, n->stream>>>(n->dA, n->z[l - 1], na, dZ_prev);
+    } else if (launch_gemm(n, EPI_GELU_BACK, dZ, out, 1, W, in, 1, batch, in, out, NULL, dZ_prev, in, n->z[l - 1])) {
+      return -2;
+    }
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
@@ -377,6 +576,11 @@ lbib_mlp* lbib_mlp_create(int n_layers, const int* widths, int max_batch, unsign
     nw += (long)n->wp[l + 1] * n->wp[l];
   }
   n->np = np;
+  n->maxw = maxw;
+  {
+    const char* e = getenv("LBIB_MLP_LEGACY");
+    n->legacy = e && e[0] == '1';
+  }
   if (!rc && cudaStreamCreateWithFlags(&n->own_stream, cudaStreamNonBlocking) != cudaSuccess) rc = -2;
   n->stream = n->own_stream;
   const size_t fp = sizeof(float) * np;
@@ -391,9 +595,19 @@ lbib_mlp* lbib_mlp_create(int n_layers, const int* widths, int max_batch, unsign
   for (int l = 0; l < L && !rc; ++l)
     if (cudaMalloc(&n->z[l], sizeof(float) * max_batch * n->wp[l + 1]) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&n->dA, sizeof(float) * max_batch * maxw) != cudaSuccess) rc = -5;
-  if (!rc && cudaMalloc(&n->dZ, sizeof(__nv_bfloat16) * max_batch * maxw) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&n->dZ, sizeof(__nv_bfloat16) * 2 * max_batch * maxw) != cudaSuccess) rc = -5;
+  /* split-K partials: up to kMaxSplit copies of the largest weight matrix */
+  n->ws_elems = 0;
+  for (int l = 0; l < L; ++l)
+    if ((long)n->wp[l + 1] * n->wp[l] > n->ws_elems) n->ws_elems = (long)n->wp[l + 1] * n->wp[l];
+  n->ws_elems *= kMaxSplit;
+  if (!rc && cudaMalloc(&n->ws, sizeof(float) * n->ws_elems) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&n->tile_cnt, sizeof(int) * kMaxTiles) != cudaSuccess) rc = -5;
+  if (!rc && cudaMemset(n->tile_cnt, 0, sizeof(int) * kMaxTiles) != cudaSuccess) rc = -2;
   if (!rc && cudaMalloc(&n->part, sizeof(float) * ((long)max_batch * maxw / 256 + 2)) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&n->d_loss, sizeof(float)) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&n->d_err, sizeof(int)) != cudaSuccess) rc = -5;
+  if (!rc && cudaMemset(n->d_err, 0, sizeof(int)) != cudaSuccess) rc = -2;
   if (!rc) {
     /* He-uniform weights for the GELU layers (bound sqrt(6 / fan_in)),
        zero biases, zero padding */
@@ -433,7 +647,8 @@ void lbib_mlp_free(lbib_mlp* n) {
   cudaFree(n->p); cudaFree(n->g); cudaFree(n->m); cudaFree(n->v); cudaFree(n->wmap); cudaFree(n->wbf);
   for (int l = 0; l <= n->L && n->act; ++l) cudaFree(n->act[l]);
   for (int l = 0; l < n->L && n->z; ++l) cudaFree(n->z[l]);
-  cudaFree(n->dA); cudaFree(n->dZ); cudaFree(n->part); cudaFree(n->d_loss);
+  cudaFree(n->dA); cudaFree(n->dZ); cudaFree(n->part); cudaFree(n->d_loss); cudaFree(n->d_err);
+  cudaFree(n->ws); cudaFree(n->tile_cnt);
   if (n->own_stream) cudaStreamDestroy(n->own_stream);
   free(n->w); free(n->wp); free(n->woff); free(n->boff); free(n->wbo); free(n->act); free(n->z);
   free(n);
@@ -483,7 +698,7 @@ int lbib_mlp_forward(lbib_mlp* n, const float* X, int batch, float* Y) {
   if (cudaMemcpy2DAsync(Y, sizeof(float) * n->w[L], n->z[L - 1], sizeof(float) * n->wp[L], sizeof(float) * n->w[L],
                         batch, cudaMemcpyDeviceToDevice, n->stream) != cudaSuccess)
     return LBIB_E_CUDA;
-  return cudaStreamSynchronize(n->stream) == cudaSuccess ? LBIB_OK : LBIB_E_CUDA;
+  return lbib_mlp_synchronize(n);
 }
 
 /* Loss and gradient (ABI order, host array of lbib_mlp_param_count floats)
@@ -498,6 +713,7 @@ int lbib_mlp_gradient(lbib_mlp* n, const float* X, const float* T, int batch, fl
       (loss && cudaMemcpyAsync(loss, n->d_loss, sizeof(float), cudaMemcpyDeviceToHost, n->stream) != cudaSuccess) ||
       cudaStreamSynchronize(n->stream) != cudaSuccess)
     rc = LBIB_E_CUDA;
+  if (!rc) rc = lbib_mlp_synchronize(n);
   if (!rc && grad) for_each_param(n, [&](long a, long i) { grad[a] = hg[i]; });
   free(hg);
   return rc;
@@ -523,9 +739,15 @@ int lbib_mlp_train_step(lbib_mlp* n, const float* X, const float* T, int batch, 
   return LBIB_OK;
 }
 
+/* Waits for the MLP's work; LBIB_E_CUDA also when a tensor-core GEMM
+ * gave up waiting on its mbarrier (its output tile was not written). */
 int lbib_mlp_synchronize(lbib_mlp* n) {
   if (!n) return LBIB_E_ARG;
-  return cudaStreamSynchronize(n->stream) == cudaSuccess ? LBIB_OK : LBIB_E_CUDA;
+  int e = 0;
+  if (cudaMemcpyAsync(&e, n->d_err, sizeof(int), cudaMemcpyDeviceToHost, n->stream) != cudaSuccess ||
+      cudaStreamSynchronize(n->stream) != cudaSuccess)
+    return LBIB_E_CUDA;
+  return e ? LBIB_E_CUDA : LBIB_OK;
 }
 
 }  /* extern "C" */

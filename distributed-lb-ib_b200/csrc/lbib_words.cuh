@@ -124,6 +124,27 @@ struct Word {
   }
 };
 
+/* Division of n < 2^31 by a fixed d in [1, 2^31) with one multiply-high and
+ * one add (the round-up method for invariant divisors, Granlund and
+ * Montgomery 1994): l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+ * n / d = (umulhi(n, m) + n) >> l.  The kernels' thread indices are below
+ * 2^31, and a 64-bit division costs tens of instructions per thread. */
+struct FastDiv {
+  unsigned d, m, l;
+};
+
+__host__ __forceinline__ FastDiv fast_div(unsigned d) {
+  FastDiv f;
+  unsigned l = 0;
+  while ((1ull << l) < d) ++l;
+  f.d = d;
+  f.l = l;
+  f.m = (unsigned)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+  return f;
+}
+
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) { return (__umulhi(n, f.m) + n) >> f.l; }
+
 template <typename T>
 struct WordsParams {
   FluidParamsT<T> p;
@@ -133,6 +154,7 @@ struct WordsParams {
   int gpr;      /* threads per row: ngroups (rows packed end to end) */
   int g0, g1;   /* groups whose cells all lie in [4, nx-5] */
   long pf;      /* L2 prefetch distance in blocks (0: none) */
+  FastDiv dgpr, dnry;  /* division by gpr and by nry */
 };
 
 /* Where a thread's V cells sit and what it does with them. */
@@ -149,19 +171,28 @@ __device__ __forceinline__ bool group_here(const WordsParams<T>& b, int g, int y
   return g >= b.g0 && g <= b.g1 && b.p.slot_cur[tile_of(g * V, y, z, b.p.ntx, b.p.nty)] < 0;
 }
 
+/* t < 2^31 (the launchers check it).  A row's first and last words are
+ * never active, so the neighbouring words' flags are the neighbouring
+ * lanes' own, also across the end of a row; only lanes 0 and 31 look
+ * theirs up. */
 template <typename T, int V>
 __device__ __forceinline__ ItemCtx item_ctx(const WordsParams<T>& b, long t) {
   ItemCtx c;
-  const long r = t / b.gpr;
-  const int g = (int)(t - r * b.gpr);
-  const bool inrow = r < b.nrows;
-  c.y = 3 + (int)(r % b.nry);
-  c.z = 3 + (int)(r / b.nry);
+  const unsigned tu = (unsigned)t;
+  const unsigned r = fdiv(tu, b.dgpr);
+  const int g = (int)(tu - r * (unsigned)b.gpr);
+  const bool inrow = r < (unsigned long)b.nrows;
+  const unsigned rz = fdiv(r, b.dnry);
+  c.y = 3 + (int)(r - rz * (unsigned)b.nry);
+  c.z = 3 + (int)rz;
   c.x0 = g * V;
   c.loads = inrow && g < b.ngroups;
   c.active = inrow && group_here<T, V>(b, g, c.y, c.z);
-  c.left_active = inrow && group_here<T, V>(b, g - 1, c.y, c.z);
-  c.right_active = inrow && group_here<T, V>(b, g + 1, c.y, c.z);
+  const int lane = threadIdx.x & 31;
+  c.left_active = __shfl_up_sync(0xffffffffu, c.active, 1);
+  c.right_active = __shfl_down_sync(0xffffffffu, c.active, 1);
+  if (lane == 0) c.left_active = inrow && group_here<T, V>(b, g - 1, c.y, c.z);
+  if (lane == 31) c.right_active = inrow && group_here<T, V>(b, g + 1, c.y, c.z);
   c.row = ((long)c.z * b.p.ny + c.y) * b.p.nx;
   return c;
 }
@@ -310,7 +341,7 @@ __device__ __forceinline__ void words_collide_store(const FluidParamsT<T>& p, co
       if (p.first || sp >= 0) {
         Mom<float> m0, m1;
         if (p.first) {
-          Fm::initial(p, m0);
+          Fm::initial_bulk(p, m0);
           m1 = m0;
         } else {
           Fm::from_tile(p, p.Uprev + (long)sp * 256, c0 + e, m0);
@@ -406,6 +437,143 @@ __device__ __forceinline__ void words_item(const WordsParams<T>& b, long t) {
   words_collide_store<T, V, PAR>(p, c, lane, d);
 }
 
+/* ---- the word step with its loads staged in shared memory by TMA ----
+ *
+ * 16-bit storage, V = 4.  The flattened (bulk row, word) space is cut into
+ * items of 128 threads: one 128-word segment of a row when a row has at
+ * least 128 words (W = nx / 4), else K = 128 / W whole rows.  A persistent
+ * CTA walks its items; one thread keeps STAGES items ahead of the compute
+ * with 1-D bulk copies (cp.async.bulk, no multicast) of every plane's row
+ * window -- the segment's cells plus 8 on either side, which covers the
+ * odd step's x shifts and keeps both ends 16-byte aligned -- into shared
+ * memory, completing on the stage's mbarrier.  The threads then read their
+ * words from shared memory (an x-shifted word from two aligned ones), so
+ * no register holds data in flight and no thread waits on DRAM; the
+ * collision and the stores (pushes assembled across lanes) are the plain
+ * word kernel's.  Only the slots a cell reads are used, and the AA rule
+ * makes those slots read and written by that cell alone, so loading an
+ * item several items ahead of the stores of this launch is safe. */
+struct TmaGeom {
+  int W;        /* words per row                                  */
+  int segw;     /* words per item segment: min(W, 128)             */
+  int K;        /* rows per item (1 when W >= 128)                 */
+  int nchunk;   /* segments per row (1 when W <= 128)              */
+  long nitems;
+  int win;      /* elements per (plane, row) window: 4 segw + 16   */
+};
+
+__host__ __forceinline__ bool tma_geometry(TmaGeom& g, int nx, long nrows) {
+  if (nx % 8) return false;
+  g.W = nx / 4;
+  if (g.W >= 128) {
+    g.segw = 128; g.K = 1; g.nchunk = (g.W + 127) / 128;
+    g.nitems = nrows * g.nchunk;
+  } else {
+    if (128 % g.W) return false;
+    g.segw = g.W; g.K = 128 / g.W; g.nchunk = 1;
+    g.nitems = (nrows + g.K - 1) / g.K;
+  }
+  g.win = 4 * g.segw + 16;
+  return true;
+}
+
+__host__ __device__ __forceinline__ int tma_stage_bytes(const TmaGeom& g) { return 19 * g.K * g.win * 2; }
+
+constexpr long kTmaSpin = 1L << 24;   /* mbarrier polls before a wait gives up */
+
+__device__ __forceinline__ uint32_t cta_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+/* Item `it`: its first bulk row and the first word of its segment. */
+__device__ __forceinline__ void tma_item(const TmaGeom& g, long it, long& row0, int& w0) {
+  if (g.nchunk > 1) { row0 = it / g.nchunk; w0 = (int)(it - row0 * g.nchunk) * 128; }
+  else { row0 = it * g.K; w0 = 0; }
+}
+
+/* Issue the bulk copies of item `it` into `stage` (one thread).  Every
+ * window stays inside its plane by construction (bulk rows have whole rows
+ * on either side); were one not to, the item's copies are not issued, the
+ * stage's barrier is released without them and err[0] is set, so that the
+ * launch reports failure instead of reading outside the buffer. */
+template <typename T, int PAR>
+__device__ __forceinline__ void tma_issue(const WordsParams<T>& b, const TmaGeom& g, long it, uint8_t* stage,
+                                          uint64_t* full, int* err) {
+  long row0;
+  int w0;
+  tma_item(g, it, row0, w0);
+  const FluidParamsT<T>& p = b.p;
+  const uint16_t* F = reinterpret_cast<const uint16_t*>(p.f);
+  const long sy = p.nx, sz = (long)p.nx * p.ny;
+  int nr = g.K;
+  if (row0 + nr > b.nrows) nr = (int)(b.nrows - row0);
+  const uint32_t bytes = (uint32_t)g.win * 2;
+  bool inside = true;
+  for (int k = 0; k < nr; ++k) {
+    const long r = row0 + k;
+    const int y = 3 + (int)(r % b.nry), z = 3 + (int)(r / b.nry);
+    const long row = ((long)z * p.ny + y) * p.nx + 4L * w0 - 8;
+    inside = inside && row - sz - sy >= 0 && row + sz + sy + g.win <= p.N;
+  }
+  if (!inside) {
+    atomicExch(err, 1);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cta_smem(full)), "r"(0u) : "memory");
+    return;
+  }
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cta_smem(full)),
+               "r"(bytes * 19u * (uint32_t)nr)
+               : "memory");
+  for (int k = 0; k < nr; ++k) {
+    const long r = row0 + k;
+    const int y = 3 + (int)(r % b.nry), z = 3 + (int)(r / b.nry);
+    const long row = ((long)z * p.ny + y) * p.nx + 4L * w0 - 8;
+#pragma unroll 1
+    for (int q = 0; q < 19; ++q) {
+      const uint16_t* src = PAR ? F + opp(q) * p.N + row - cy(q) * sy - cz(q) * sz : F + q * p.N + row;
+      uint8_t* dst = stage + ((long)q * g.K + k) * bytes;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              cta_smem(dst)),
+          "l"(src), "r"(bytes), "r"(cta_smem(full))
+          : "memory");
+    }
+  }
+}
+
+__device__ __forceinline__ bool tma_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = cta_smem(bar);
+  for (long i = 0; i < kTmaSpin; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+/* The incoming word of direction q for the thread's cells from the staged
+ * window (element e0 = the thread's first cell). */
+template <int PAR>
+__device__ __forceinline__ Word<__half, 4> smem_word(const uint16_t* w, int e0, int q) {
+  Word<__half, 4> o;
+  const uint2 m = *reinterpret_cast<const uint2*>(w + e0);
+  if (PAR == 0 || cx(q) == 0) {
+    o.r[0] = m.x; o.r[1] = m.y;
+  } else if (cx(q) == 1) {
+    const uint32_t l = *reinterpret_cast<const uint32_t*>(w + e0 - 2);
+    o.r[0] = __byte_perm(l, m.x, 0x5432);
+    o.r[1] = __byte_perm(m.x, m.y, 0x5432);
+  } else {
+    const uint32_t h = *reinterpret_cast<const uint32_t*>(w + e0 + 4);
+    o.r[0] = __byte_perm(m.x, m.y, 0x5432);
+    o.r[1] = __byte_perm(m.y, h, 0x5432);
+  }
+  return o;
+}
+
 /* A cell of a forced tile inside the word kernel's range (bulk rows,
  * x in [4, nx-5]; zb = last bulk z row), by the generic per-cell rules. */
 template <typename T, int PAR>
@@ -472,6 +640,8 @@ __host__ __forceinline__ void words_geometry(WordsParams<T>& b, int V, int nx, i
   b.g0 = (4 + V - 1) / V;
   b.g1 = (nx - 4) / V - 1;
   b.pf = 0;
+  b.dgpr = fast_div((unsigned)b.gpr);
+  b.dnry = fast_div((unsigned)(nry > 0 ? nry : 1));
 }
 
 }  // namespace lbib

@@ -36,8 +36,10 @@ __device__ __forceinline__ void x2_relax_cell(const FluidParams& p, int x, int y
   const int tile = tile_of(x, y, z, p.ntx, p.nty);
   const int cell = cell_in_tile(x, y, z);
   double rho, ux, uy, uz;
-  if (plane || p.first) {
+  if (plane) {
     rho = p.rho0; ux = p.ux0; uy = 0.0; uz = 0.0;
+  } else if (p.first) {
+    rho = p.rho0; ux = p.ux_rest; uy = 0.0; uz = 0.0;
   } else {
     const int sp = p.slot_prev[tile];
     if (sp >= 0) {

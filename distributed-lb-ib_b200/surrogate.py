@@ -288,10 +288,57 @@ def evaluate(model, problems, steps: int, truth=None, thresholds=None, rerun_pre
             "all_completed_tip_within_2pct_frac": float((rel[true_alive] <= 0.02).mean()) if true_alive.any() else None}
 
 
+def pipeline(train_n: int = 4096, eval_n: int = 2048, steps: int = 3000, every: int = 100, iters: int = 10000,
+             members: int = 3, calib_frac: float = 0.125, target: float = 0.98,
+             rerun_precision: str = "f16-flow", data: str = None) -> Dict:
+    """The whole learned sweep: training runs (batched, FP16 storage), GPU
+    training, calibration of the re-run thresholds on the last `calib_frac`
+    of the training runs, the plain FP64 batched sweep of the held-out points
+    (the judge, and the baseline rate), and the screen of the same points.
+    With `data`, simulated runs are kept there and reused."""
+    import os
+    out = {"config": {"train_n": train_n, "eval_n": eval_n, "steps": steps, "every": every, "iters": iters,
+                      "members": members, "calib_frac": calib_frac, "target": target,
+                      "rerun_precision": rerun_precision}}
+    tr = draw(train_n, 2)
+    ev = draw(eval_n, 3)
+    ftr = os.path.join(data, f"train_{train_n}_{steps}_{every}.npz") if data else None
+    fev = os.path.join(data, f"truth_{eval_n}_{steps}.npz") if data else None
+    if ftr and os.path.exists(ftr):
+        z = np.load(ftr)
+        disp, alive, gen_s = z["disp"].astype(np.float32), z["alive"], float(z["seconds"])
+    else:
+        disp, alive, _, gen_s = simulate(tr, steps, every, "f16-flow")
+        if ftr:
+            os.makedirs(data, exist_ok=True)
+            np.savez(ftr, disp=disp.astype(np.float16), alive=alive, seconds=gen_s)
+    out["training_runs"] = {"n": train_n, "seconds": gen_s, "completed": int(clean(disp, alive)[1][:, -1].sum())}
+    nval = max(1, int(round(train_n * calib_frac)))      # the last runs calibrate the screen
+    ntr = train_n - nval
+    X, Y = training_set(tr[:ntr], disp[:ntr], alive[:ntr])
+    t0 = time.perf_counter()
+    model, curves = train(X, Y, members=members, iters=iters)
+    out["training"] = {"runs": ntr, "samples": int(X.shape[0]), "seconds": time.perf_counter() - t0,
+                       "loss_curves": curves}
+    dv, okv = clean(disp[ntr:], alive[ntr:])
+    th = calibrate(model, tr[ntr:], dv[:, -1], okv[:, -1], target=target)
+    out["calibration"] = dict(th, runs=nval)
+    if fev and os.path.exists(fev):
+        z = np.load(fev)
+        truth = (z["disp"], z["alive"], z["stop"], float(z["seconds"]))
+    else:
+        truth = simulate(ev, steps, steps, "f64")
+        if fev:
+            np.savez(fev, disp=truth[0], alive=truth[1], stop=truth[2], seconds=truth[3])
+    out["evaluation"] = evaluate(model, ev, steps, truth=truth, thresholds=th, rerun_precision=rerun_precision)
+    for n in model[0] + [model[1]]:
+        n.close()
+    return out
+
+
 def main(argv=None) -> int:
     import argparse
     import json
-    import os
 
     ap = argparse.ArgumentParser(description="learned sweep screen")
     ap.add_argument("--train-n", type=int, default=4096)
@@ -299,48 +346,19 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--iters", type=int, default=10000)
+    ap.add_argument("--members", type=int, default=3)
+    ap.add_argument("--calib-frac", type=float, default=0.125,
+                    help="fraction of the training runs held back to calibrate the re-run thresholds")
+    ap.add_argument("--target", type=float, default=0.98,
+                    help="rate of right points the calibration asks of the points the surrogate reports")
     ap.add_argument("--rerun-precision", default="f16-flow",
                     help="storage of the batched solver that re-runs the flagged points (f64: the plain solver)")
     ap.add_argument("--data", default=None,
                     help="directory to keep the simulated runs in (reused when present: only the "
                          "training and the screen run again)")
     a = ap.parse_args(argv)
-    out = {}
-    tr = draw(a.train_n, 2)
-    ev = draw(a.eval_n, 3)
-    ftr = os.path.join(a.data, "train.npz") if a.data else None
-    fev = os.path.join(a.data, "truth.npz") if a.data else None
-    if ftr and os.path.exists(ftr):
-        z = np.load(ftr)
-        disp, alive, gen_s = z["disp"].astype(np.float32), z["alive"], float(z["seconds"])
-    else:
-        disp, alive, _, gen_s = simulate(tr, a.steps, a.every, "f16-flow")
-        if ftr:
-            os.makedirs(a.data, exist_ok=True)
-            np.savez(ftr, disp=disp.astype(np.float16), alive=alive, seconds=gen_s)
-    out["training_runs"] = {"n": a.train_n, "seconds": gen_s, "completed": int(clean(disp, alive)[1][:, -1].sum())}
-    nval = a.train_n // 8                      # the last runs calibrate the screen
-    ntr = a.train_n - nval
-    X, Y = training_set(tr[:ntr], disp[:ntr], alive[:ntr])
-    t0 = time.perf_counter()
-    model, curves = train(X, Y, iters=a.iters)
-    out["training"] = {"runs": ntr, "samples": int(X.shape[0]), "seconds": time.perf_counter() - t0,
-                       "loss_curves": curves}
-    dv, okv = clean(disp[ntr:], alive[ntr:])
-    th = calibrate(model, tr[ntr:], dv[:, -1], okv[:, -1])
-    out["calibration"] = dict(th, runs=nval)
-    truth = None
-    if fev and os.path.exists(fev):
-        z = np.load(fev)
-        truth = (z["disp"], z["alive"], z["stop"], float(z["seconds"]))
-    else:
-        truth = simulate(ev, a.steps, a.steps, "f64")
-        if fev:
-            np.savez(fev, disp=truth[0], alive=truth[1], stop=truth[2], seconds=truth[3])
-    out["evaluation"] = evaluate(model, ev, a.steps, truth=truth, thresholds=th,
-                                 rerun_precision=a.rerun_precision)
-    for n in model[0] + [model[1]]:
-        n.close()
+    out = pipeline(a.train_n, a.eval_n, a.steps, a.every, a.iters, a.members, a.calib_frac, a.target,
+                   a.rerun_precision, a.data)
     print(json.dumps(out))
     return 0
 

@@ -262,6 +262,25 @@ void save_fiber_sub_grid_cord_ef_use_fv(GV gv, int start_y, int start_z, int end
  * (mpi/init_gv.c:74-97).  Call before init_gv / init_eqlbrmdistrfuncDF0:
  * it also resets the initial velocity to (u_l, 0, 0). */
 int lbib_set_params(GV gv, double tau, double u_l, double Ks_l, double Kb_l);
+/* The LBIB_COMPAT_* bits below, and the option bits LBIB_OPT_* (physics the
+ * benchmark workloads describe and the reference does not have; their
+ * parity is pinned to the CPU restatement only).  Call before init_gv;
+ * lbib_case_create* take the same word as their compat argument:
+ *   LBIB_OPT_PERIODIC_Z  z is periodic over the fluid interior (period
+ *                        nz - 4) and only the y = 2, ny-3 walls bounce back;
+ *                        the reference's periodicBC (mpi/periodicBC.c:29-134)
+ *                        is never called by its step loop
+ *   LBIB_OPT_REST_START  the cells x in [3, nx-4] start at u = 0 (f = f_eq
+ *                        with rho = 1); the inlet/outlet planes and their
+ *                        fixed tables keep the inflow (1, u_l), which then
+ *                        drives the channel (the reference starts every cell
+ *                        at (u_l, 0, 0), mpi/gen_fluid_grid.c:61-64)
+ *   LBIB_OPT_PIN_ROW0    row 0 of every sheet stays where it is (the
+ *                        reference's tethering loops are no-ops,
+ *                        cube_pthread/lbm_ib.c:909-917) */
+#define LBIB_OPT_PERIODIC_Z  0x100
+#define LBIB_OPT_REST_START  0x200
+#define LBIB_OPT_PIN_ROW0    0x400
 int lbib_set_compat(GV gv, int flags);
 /* Selects the population storage (LBIB_PREC_*); init_gv_constant sets F64.
  * Call before init_gv: when the grid's GPU state exists it is rebuilt in

@@ -156,6 +156,15 @@ orc_state* orc_create(int nx, int ny, int nz, int cube_size, int nsheets,
   for (long i = 0; i < N; ++i) {
     s->rho[i] = s->rho_l; s->ux[i] = s->u_l; s->uy[i] = 0.0; s->uz[i] = 0.0;
   }
+  /* rest start: the cells whose moments the step updates, x in [3, nx-4],
+     start at u = 0; the plane cells x = 2, nx-3 (whose rho, u the reference
+     never recomputes) and the cells the inlet/outlet tables are taken from
+     keep the inflow (1, u_l), so the channel is driven from the planes */
+  if (compat & ORC_OPT_REST_START)
+    for (long i = 0; i < N; ++i) {
+      const int x = (int)(i % nx);
+      if (x >= 3 && x <= nx - 4) s->ux[i] = 0.0;
+    }
   for (long i = 0; i < N; ++i)
     for (int q = 0; q < 19; ++q)
       s->dfeq[q * N + i] = orc_feq(s, q, s->rho[i], s->ux[i], s->uy[i], s->uz[i]);
@@ -419,13 +428,19 @@ void orc_collide(orc_state* s) {
  * df2 at x + c_q <- df1 at x, for every source x in [2, n-3]^3. */
 void orc_stream(orc_state* s) {
   const long N = s->N;
+  const int periodic = (s->compat & ORC_OPT_PERIODIC_Z) != 0, nz = s->nz;
 #pragma omp parallel for schedule(static)
   for (int z = 2; z <= s->nz - 3; ++z)
     for (int y = 2; y <= s->ny - 3; ++y)
       for (int x = 2; x <= s->nx - 3; ++x) {
         long i = IDX(s, x, y, z);
         for (int q = 0; q < 19; ++q) {
-          long t = IDX(s, x + (int)s->c[q][0], y + (int)s->c[q][1], z + (int)s->c[q][2]);
+          int zt = z + (int)s->c[q][2];
+          /* periodic option: a link leaving I in z re-enters at the other
+             side (period nz - 4, the z extent of I) */
+          if (periodic && zt < 2) zt += nz - 4;
+          if (periodic && zt > nz - 3) zt -= nz - 4;
+          long t = IDX(s, x + (int)s->c[q][0], y + (int)s->c[q][1], zt);
           s->df2[q * N + t] = s->df1[q * N + i];
         }
       }
@@ -439,6 +454,17 @@ void orc_bounceback(orc_state* s) {
   const int cs = s->cs, ncx = s->ncx, ncy = s->ncy, ncz = s->ncz;
   const int xlo = 3, xhi = s->nx - 4;
 #define BB(dst, src) s->df2[(dst) * N + i] = s->df1[(src) * N + i]
+  if (s->compat & ORC_OPT_PERIODIC_Z) {
+    /* periodic option: no z walls; the y walls over the whole z extent of I */
+    for (int z = 2; z <= s->nz - 3; ++z)
+      for (int x = xlo; x <= xhi; ++x) {
+        long i = IDX(s, x, 2, z);
+        BB(6, 5); BB(12, 11); BB(13, 14); BB(16, 15); BB(17, 18);
+        i = IDX(s, x, s->ny - 3, z);
+        BB(5, 6); BB(11, 12); BB(14, 13); BB(15, 16); BB(18, 17);
+      }
+    return;
+  }
   /* z walls: z = kb and z = ke, x in [ib+1, ie-1], y in [jb, je] */
   for (int x = xlo; x <= xhi; ++x)
     for (int y = 2; y <= s->ny - 3; ++y) {
@@ -523,8 +549,10 @@ int orc_move(orc_state* s) {
   for (int k = 0; k < s->nsheets; ++k) {
     orc_sheet* sh = &s->sheets[k];
     long n = (long)sh->rows * sh->cols;
+    /* pinned-row option: row 0 (the first cols nodes) stays where it is */
+    const long a0 = (s->compat & ORC_OPT_PIN_ROW0) ? sh->cols : 0;
 #pragma omp parallel for schedule(static) reduction(|: err)
-    for (long a = 0; a < n; ++a) {
+    for (long a = a0; a < n; ++a) {
       double* m = sh->node + a * 12;
       double s1 = 0, s2 = 0, s3 = 0;
       int is = (int)(floor(m[0] * dx1 - 2) + 1);

@@ -24,6 +24,13 @@ extern "C" {
 #define ORC_COMPAT_INOUT_PTHREAD  4  /* lbm_ib.c:2800-2882 loop BK < num_cubes_x, serial */
 #define ORC_COMPAT_ALL            7
 
+/* Options with no reference counterpart (the workload definitions ask for
+ * them; the reference has none of them, so their parity is unpinned beyond
+ * this restatement).  They ride in the same word as the compat bits. */
+#define ORC_OPT_PERIODIC_Z   0x100  /* z periodic over I, walls only at y            */
+#define ORC_OPT_REST_START   0x200  /* interior starts at u = 0; inflow on the planes */
+#define ORC_OPT_PIN_ROW0     0x400  /* row 0 of every sheet does not move            */
+
 typedef struct orc_state orc_state;
 
 orc_state* orc_create(int nx, int ny, int nz, int cube_size, int nsheets,

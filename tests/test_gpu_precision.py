@@ -109,11 +109,18 @@ def test_precision_switch_rebuilds_state(gpu):
 
 
 # cases for the word kernel: rows of 3+ warps (lane 0 / 31 crossings), a row
-# of one active word (nx = 12), forcing tiles at the row ends
+# of one active word (nx = 12), forcing tiles at the row ends; for the
+# TMA-staged variants, items of 16 rows (nx = 32), of 8 rows (nx = 64), of
+# exactly one row (nx = 512) and rows of two segments, the second partial
+# (nx = 640); rows whose word count does not divide 128 (nx = 160, 12) fall
+# back to the plain word kernel
 WORD_CASES = {
     "long_rows": (small_case(160, 12, 12, 6, 6, 20.0), 9),
     "short_rows": (small_case(12, 12, 24, 6, 6, 5.0), 7),
     "sheet_at_inlet": (small_case(32, 16, 16, 8, 8, 4.5), 9),
+    "eight_row_items": (small_case(64, 16, 20, 8, 8, 10.0), 8),
+    "one_row_items": (small_case(512, 12, 16, 6, 6, 40.0), 7),
+    "two_segment_rows": (small_case(640, 12, 12, 6, 6, 20.0), 7),
 }
 # rounding-level differences only: FMA contraction may differ between the
 # two kernels, which moves a 16-bit value by at most an ulp now and then
