@@ -618,6 +618,7 @@ lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision
       d->Utile[c] = b->Utile[c];
     }
     d->stream = b->stream;
+    d->fluid_stream = b->stream;
     d->err = b->err + 2 * k;
     d->use_bulk = b->h_desc[k].bulk;
     d->have_df1 = d->have_inout = 1;

@@ -5,9 +5,13 @@
  * Why: the reference evaluates (1 + cos(pi/2 * r)) with the host C library
  * (cube_pthread/lbm_ib.c:1447, :2679-2683).  The LBM-IB run amplifies a
  * last-bit difference in any weight to ~1e-10 relative after ~1000 steps, so
- * the CUDA path needs the same cosine values bit for bit.  glibc's cos is
- * correctly rounded on this argument range in practice (checked against this
- * function by tests/test_cos.py); CUDA's cos carries a 2-ulp bound.  This is
+ * the CUDA path needs cosine values that a CPU oracle can reproduce bit for
+ * bit.  glibc's cos is not correctly rounded: on this argument range about
+ * 0.13% of its values are 1 ulp off (tests/test_cos.py shows such cases), and
+ * CUDA's cos carries a 2-ulp bound, so neither can be matched exactly by the
+ * other.  A correctly rounded cosine is reproducible anywhere: the CUDA path
+ * and the oracle built with this function agree bit for bit, and both stay
+ * within 1e-10 of the reference's glibc-based run.  This is
  * not CUDA's algorithm: it is the double-double method of Dekker (1971) and
  * Knuth (TAOCP vol. 2, TwoSum) as used by the QD library (Hida, Li & Bailey,
  * 2001): reduce by k*pi/2 with a triple-double pi/2, then evaluate the Taylor

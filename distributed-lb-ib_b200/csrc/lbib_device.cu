@@ -24,6 +24,8 @@ int lbdev_lp_variants(int prec);
 int lbdev_launch_fiber_forces(lbib_device* d, int k);
 int lbdev_launch_spread(lbib_device* d, int step);
 int lbdev_launch_move(lbib_device* d);
+int lbdev_launch_stencil_box(lbib_device* d);
+int lbdev_launch_box_cells(lbib_device* d);
 int lbdev_launch_scatter_force(lbib_device* d, double* fx, double* fy, double* fz);
 }
 
@@ -195,7 +197,12 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   d->ncx = c->nx / c->cube_size; d->ncy = c->ny / c->cube_size; d->ncz = c->nz / c->cube_size;
   lbdev_set_physics(d, c);
   cudaGetDevice(&d->device);
-  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) { free(d); return -2; }
+  /* the state's stream gets the highest priority: in an overlapped step the
+     spread's short kernels then take SMs ahead of the bulk fluid kernel,
+     which runs on the low-priority side stream */
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if (cudaStreamCreateWithPriority(&d->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess) { free(d); return -2; }
   d->ntx = (d->nx + 3) / 4; d->nty = (d->ny + 3) / 4; d->ntz = (d->nz + 3) / 4;
   d->ntiles = (long)d->ntx * d->nty * d->ntz;
   int rc = 0;
@@ -216,6 +223,19 @@ extern "C" int lbdev_create(lbib_device** out, const lbdev_config* c) {
   d->lp_variant = -1;
   const char* pf = getenv("LBIB_L2_PREFETCH");
   d->l2_pf = pf ? atoi(pf) : 0;
+  d->fluid_stream = d->stream;
+  /* box-mode steps for a whole grid: 1 in stream order (default), 2 with
+     the fluid's bulk concurrent to the spread, 0 off (LBIB_OVERLAP) */
+  const char* ov = getenv("LBIB_OVERLAP");
+  d->overlap = (d->x_lo == 0 && d->x_hi == d->nx) ? (ov ? atoi(ov) : 1) : 0;
+  if (d->overlap &&
+      (cudaStreamCreateWithPriority(&d->side, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+       cudaEventCreateWithFlags(&d->ev_box, cudaEventDisableTiming) != cudaSuccess ||
+       cudaEventCreateWithFlags(&d->ev_bulk, cudaEventDisableTiming) != cudaSuccess ||
+       cudaMalloc(&d->box, sizeof(int) * 12) != cudaSuccess)) {
+    lbdev_free(d);
+    return -2;
+  }
   *out = d;
   return 0;
 }
@@ -270,14 +290,20 @@ extern "C" void lbdev_free(lbib_device* d) {
   cudaFree(d->halo);
   cudaFree(d->scratch);
   for (int i = 0; i < d->nhost_reg; ++i) cudaHostUnregister(d->host_reg[i]);
-  for (long i = 0; i < 6 * d->prof_cap; ++i) cudaEventDestroy(d->prof_ev[i]);
+  for (long i = 0; i < LBIB_PROF_EV * d->prof_cap; ++i) cudaEventDestroy(d->prof_ev[i]);
   free(d->prof_ev);
+  free(d->prof_overlap);
   if (d->h_err) cudaFreeHost(d->h_err);
+  if (d->side) cudaStreamDestroy(d->side);
+  if (d->ev_box) cudaEventDestroy(d->ev_box);
+  if (d->ev_bulk) cudaEventDestroy(d->ev_bulk);
+  cudaFree(d->box);
   if (d->stream) cudaStreamDestroy(d->stream);
   free(d);
 }
 
 extern "C" int lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_dev* sh, const double* nodes_host) {
+  d->box_valid = 0;
   if (nsheets < 1) return -1;
   long S = 0;
   for (int k = 0; k < nsheets; ++k) {
@@ -306,6 +332,7 @@ extern "C" int lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_de
       CK(cudaMemsetAsync(d->tile_count[b], 0, sizeof(int), d->stream));
     }
     CK(cudaMalloc(&d->tile_cnt, sizeof(int) * d->ntiles));
+    CK(cudaMemsetAsync(d->tile_cnt, 0, sizeof(int) * d->ntiles, d->stream));   /* the compaction keeps it at 0 */
     CK(cudaMalloc(&d->slot_off, sizeof(int) * d->cap));
     CK(cudaMalloc(&d->slot_len, sizeof(int) * d->cap));
     CK(cudaMalloc(&d->slot_cursor, sizeof(int) * d->cap));
@@ -336,6 +363,7 @@ extern "C" int lbdev_init_equilibrium(lbib_device* d) {
 }
 
 extern "C" int lbdev_init_df1(lbib_device* d) {
+  d->box_valid = 0;
   if (lbdev_launch_init(d, 0)) return -2;
   d->parity = 0;
   d->steps = 0;
@@ -355,6 +383,8 @@ extern "C" int lbdev_init_inout(lbib_device* d) {
 
 extern "C" int lbdev_stage(lbib_device* d, int which, int step_no) {
   if (!d->nodes || !d->have_df1 || !d->have_inout) return -4;
+  d->box_valid = 0;   /* stage-by-stage calls may move the sheet */
+  d->box_next = NULL;
   switch (which) {
     case 0:
       for (int k = 0; k < d->nsheets; ++k)
@@ -390,12 +420,84 @@ extern "C" int lbdev_stage(lbib_device* d, int which, int step_no) {
 
 static int prof_grow(lbib_device* d) {
   long cap = d->prof_cap ? 2 * d->prof_cap : 256;
-  cudaEvent_t* ev = (cudaEvent_t*)realloc(d->prof_ev, sizeof(cudaEvent_t) * 6 * cap);
+  cudaEvent_t* ev = (cudaEvent_t*)realloc(d->prof_ev, sizeof(cudaEvent_t) * LBIB_PROF_EV * cap);
   if (!ev) return -5;
   d->prof_ev = ev;
-  for (long i = 6 * d->prof_cap; i < 6 * cap; ++i) CK(cudaEventCreate(&d->prof_ev[i]));
+  char* mode = (char*)realloc(d->prof_overlap, cap);
+  if (!mode) return -5;
+  d->prof_overlap = mode;
+  for (long i = LBIB_PROF_EV * d->prof_cap; i < LBIB_PROF_EV * cap; ++i) CK(cudaEventCreate(&d->prof_ev[i]));
   d->prof_cap = cap;
   return 0;
+}
+
+/* One full step in box mode (d->overlap, a whole grid): the box of this
+ * step's stencils first; the fluid step's row and bulk kernels skip the
+ * box's tiles and read no force -- they need nothing from this step's
+ * forces and spread, and they lose the per-cell force-map lookups and the
+ * forced collision from their code -- and the box's cells are stepped by
+ * the generic rules after the spread; then the tile moments and the move.
+ * Every cell is stepped once by the same per-cell arithmetic (the generic
+ * rules give the two-cell kernel's bits), so the results do not change.
+ * d->overlap == 2 runs the row and bulk kernels on the side stream,
+ * concurrently with the forces and the spread; 1 keeps one stream (the
+ * spread's kernels spread over every SM, and interleaving them with the
+ * bandwidth-bound bulk kernel measured slower than running them in turn). */
+static int step_overlapped(lbib_device* d, int step_no, cudaEvent_t* ev) {
+  if (!d->nodes || !d->have_df1 || !d->have_inout) return -4;
+  /* the box of this step's stencils: left by the previous step's move, or
+     computed here (first step, positions set from the host, pinned rows --
+     whose nodes the move does not visit) */
+  const int pinned = (d->compat & LBIB_OPT_PIN_ROW0) != 0;
+  if (!d->box_valid || pinned)
+    if (lbdev_launch_stencil_box(d)) return -2;
+  d->box_next = pinned ? NULL : d->box + 6 * (d->box_cur ^ 1);
+  CK(cudaEventRecord(d->ev_box, d->stream));
+  /* the step's buffers: the spread fills cur, the fluid reads cur ^ 1's moments */
+  d->cur ^= 1;
+  d->have_forces = 1;
+  d->have_moments = 0;
+  d->box_mode = 1;
+  const int conc = d->overlap == 2;
+  cudaStream_t fs = conc ? d->side : d->stream;
+  int rc = 0;
+  if (!conc) {
+    for (int k = 0; k < d->nsheets && !rc; ++k) rc = lbdev_launch_fiber_forces(d, k);
+    if (ev) CK(cudaEventRecord(ev[1], d->stream));
+    if (!rc) rc = lbdev_launch_spread(d, step_no);
+    if (ev) CK(cudaEventRecord(ev[2], d->stream));
+    if (rc) { d->box_mode = 0; d->box_next = NULL; d->box_valid = 0; return -2; }
+  }
+  d->fluid_stream = fs;
+  if (conc) CK(cudaStreamWaitEvent(d->side, d->ev_box, 0));
+  if (ev) CK(cudaEventRecord(ev[6], fs));
+  rc = lbdev_launch_fluid_step(d);
+  if (ev) CK(cudaEventRecord(ev[7], fs));
+  if (conc) CK(cudaEventRecord(d->ev_bulk, d->side));
+  d->fluid_stream = d->stream;
+  if (rc) { d->box_mode = 0; d->box_next = NULL; d->box_valid = 0; return -2; }
+  if (conc) {
+    for (int k = 0; k < d->nsheets && !rc; ++k) rc = lbdev_launch_fiber_forces(d, k);
+    if (ev) CK(cudaEventRecord(ev[1], d->stream));
+    if (!rc) rc = lbdev_launch_spread(d, step_no);
+    if (ev) CK(cudaEventRecord(ev[2], d->stream));
+    CK(cudaStreamWaitEvent(d->stream, d->ev_bulk, 0));
+  }
+  if (ev) CK(cudaEventRecord(ev[8], d->stream));
+  if (!rc) rc = lbdev_launch_box_cells(d);
+  d->box_mode = 0;
+  if (rc) { d->box_next = NULL; d->box_valid = 0; return -2; }
+  if (ev) CK(cudaEventRecord(ev[3], d->stream));
+  d->have_moments = 1;
+  rc = lbdev_launch_tile_moments(d) ? -2 : 0;
+  if (ev) CK(cudaEventRecord(ev[4], d->stream));
+  if (!rc) rc = lbdev_launch_move(d) ? -2 : 0;
+  if (ev) CK(cudaEventRecord(ev[5], d->stream));
+  /* the move reduced the next step's box into box_next */
+  d->box_valid = !rc && d->box_next != NULL;
+  if (d->box_valid) d->box_cur ^= 1;
+  d->box_next = NULL;
+  return rc;
 }
 
 extern "C" int lbdev_step(lbib_device* d, int step_no) {
@@ -403,15 +505,21 @@ extern "C" int lbdev_step(lbib_device* d, int step_no) {
   cudaEvent_t* ev = NULL;
   if (d->profiling) {
     if (d->prof_steps >= d->prof_cap && prof_grow(d)) return -5;
-    ev = d->prof_ev + 6 * d->prof_steps;
+    ev = d->prof_ev + LBIB_PROF_EV * d->prof_steps;
     CK(cudaEventRecord(ev[0], d->stream));
+  }
+  if (d->overlap) {
+    const int rc = step_overlapped(d, step_no, ev);
+    if (rc) return rc;
+    if (ev) d->prof_overlap[d->prof_steps++] = 1;
+    return 0;
   }
   for (int i = 0; i < 5; ++i) {
     int rc = lbdev_stage(d, order[i], step_no);
     if (rc) return rc;
     if (ev) CK(cudaEventRecord(ev[i + 1], d->stream));
   }
-  if (ev) d->prof_steps++;
+  if (ev) d->prof_overlap[d->prof_steps++] = 0;
   return 0;
 }
 
@@ -427,10 +535,18 @@ extern "C" int lbdev_profile_end(lbib_device* d, double* stage_ms, long* steps) 
   CK(cudaStreamSynchronize(d->stream));
   for (int s = 0; s < LBIB_NSTAGE_TIMED; ++s) stage_ms[s] = 0.0;
   for (long t = 0; t < d->prof_steps; ++t) {
-    cudaEvent_t* ev = d->prof_ev + 6 * t;
+    cudaEvent_t* ev = d->prof_ev + LBIB_PROF_EV * t;
     for (int s = 0; s < LBIB_NSTAGE_TIMED; ++s) {
       float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, ev[s], ev[s + 1]));
+      if (s == 2 && d->prof_overlap[t]) {
+        /* overlapped: the bulk launches (side stream) plus the box's cells */
+        float a = 0.f, b = 0.f;
+        CK(cudaEventElapsedTime(&a, ev[6], ev[7]));
+        CK(cudaEventElapsedTime(&b, ev[8], ev[3]));
+        ms = a + b;
+      } else {
+        CK(cudaEventElapsedTime(&ms, ev[s], ev[s + 1]));
+      }
       stage_ms[s] += ms;
     }
   }
@@ -557,12 +673,14 @@ extern "C" int lbdev_copy_nodes_out(lbib_device* d, long first, long n, double* 
 }
 
 extern "C" int lbdev_copy_nodes_in(lbib_device* d, long first, long n, const double* host) {
+  d->box_valid = 0;
   if (first < 0 || n < 0 || first + n > d->S) return -1;
   CK(cudaMemcpyAsync(d->nodes + 12 * first, host, sizeof(double) * 12 * n, cudaMemcpyHostToDevice, d->stream));
   return 0;
 }
 
 extern "C" int lbdev_set_nodes(lbib_device* d, const double* in) {
+  d->box_valid = 0;
   CK(cudaMemcpyAsync(d->nodes, in, sizeof(double) * 12 * d->S, cudaMemcpyHostToDevice, d->stream));
   CK(cudaStreamSynchronize(d->stream));
   return 0;
@@ -628,6 +746,7 @@ extern "C" int lbdev_save_state(lbib_device* d, FILE* fp) {
 }
 
 extern "C" int lbdev_load_state(lbib_device* d, FILE* fp) {
+  d->box_valid = 0;
   if (!d->nodes || !d->tile_slot[0]) return -4;
   CK(cudaStreamSynchronize(d->stream));
   int hdr[6];

@@ -22,6 +22,8 @@
 #define LBIB_FLUID_KERNELS_CUH
 
 #include "lbib_internal.h"
+#include <climits>
+
 #include "lbib_lattice.cuh"
 
 namespace lbib {
@@ -223,7 +225,9 @@ __device__ __forceinline__ void step_cell(const FluidParamsT<T>& p, int x, int y
     if (sp >= 0) F::from_tile(p, p.Uprev + (long)sp * 256, cell, m);
     else F::moments_free(f, p, m);
   }
-  const int sc = p.slot_cur[tile];
+  /* box mode: a cell outside the box carries no force, and this step's
+     tile map may still be under construction by the concurrent spread */
+  const int sc = (p.box && !in_box(p.box, x, y, z)) ? -1 : p.slot_cur[tile];
   if (sc >= 0) {
     const double* Ft = p.Fcur + (long)sc * 192;
     F::template collide<true>(f, m, (R)Ft[cell], (R)Ft[64 + cell], (R)Ft[128 + cell], p);
@@ -239,7 +243,37 @@ __global__ void __launch_bounds__(128, LBIB_FLUID_MINB)
   const int x = blockIdx.y * blockDim.x + threadIdx.x + p.xlo;
   const int2 r = rows[blockIdx.x];
   if (x > p.xhi) return;
+  if (p.box && in_box(p.box, x, r.x, r.y)) return;
   step_cell<T, PAR>(p, x, r.x, r.y);
+}
+
+/* Box mode: every cell of I in the tiles of the box, by the generic rules
+ * (forced where this step's spread touched the tile), one CTA of 64
+ * threads per tile, a persistent grid over the box. */
+template <typename T, int PAR>
+__global__ void __launch_bounds__(64) lbib_box_cells(FluidParamsT<T> p, int* __restrict__ reset) {
+  /* the next step's box starts empty; the move fills it (it runs after us) */
+  if (reset && blockIdx.x == 0 && threadIdx.x < 6) reset[threadIdx.x] = (threadIdx.x & 1) ? INT_MIN : INT_MAX;
+  const int* b = p.box;
+  const long lbx = (long)b[1] - b[0] + 1, lby = (long)b[3] - b[2] + 1, lbz = (long)b[5] - b[4] + 1;
+  if (lbx <= 0 || lby <= 0 || lbz <= 0) return;
+  const int nbx = (int)lbx, nby = (int)lby, nbz = (int)lbz;
+  const long n = (long)nbx * nby * nbz;
+  const int cell = threadIdx.x;
+  for (long i = blockIdx.x; i < n; i += gridDim.x) {
+    const int tx = b[0] + (int)(i % nbx), ty = b[2] + (int)((i / nbx) % nby), tz = b[4] + (int)(i / ((long)nbx * nby));
+    const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
+    if (x >= p.xlo && x <= p.xhi && y >= 2 && y <= p.ny - 3 && z >= 2 && z <= p.nz - 3) step_cell<T, PAR>(p, x, y, z);
+  }
+}
+
+template <typename T>
+int launch_box_cells_t(lbib_device* d, const FluidParamsT<T>& p) {
+  const unsigned blocks = 148 * 16;
+  if (d->parity == 0) lbib_box_cells<T, 0><<<blocks, 64, 0, d->stream>>>(p, d->box_next);
+  else lbib_box_cells<T, 1><<<blocks, 64, 0, d->stream>>>(p, d->box_next);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 /* (rho, u)(t) of cell `cell` of touched tile `tile` (slot i), after the
@@ -430,6 +464,7 @@ FluidParamsT<T> make_params_t(lbib_device* d, int first) {
   p.slot_cur = d->tile_slot[c]; p.Fcur = d->Ftile[c];
   p.slot_prev = d->tile_slot[c ^ 1]; p.Uprev = d->Utile[c ^ 1];
   p.ntx = d->ntx; p.nty = d->nty;
+  p.box = d->box_mode ? d->box + 6 * d->box_cur : nullptr;
   lbdev_shift(d, p.sh, &p.rhos, &p.uxs);
   p.frs = (float)p.rhos; p.fus = (float)p.uxs;
   p.fom = (float)p.omtau; p.fit = (float)p.invtau; p.fhdt = (float)p.half_dt; p.fg = (float)p.g;
@@ -449,8 +484,8 @@ int launch_step_rows_t(lbib_device* d, const FluidParamsT<T>& p) {
   if (d->nrows <= 0) return 0;
   dim3 block(128);
   dim3 grid((unsigned)d->nrows, (unsigned)((p.xhi - p.xlo + 1 + 127) / 128));
-  if (d->parity == 0) lbib_fluid_step<T, 0><<<grid, block, 0, d->stream>>>(p, (const int2*)d->rows);
-  else lbib_fluid_step<T, 1><<<grid, block, 0, d->stream>>>(p, (const int2*)d->rows);
+  if (d->parity == 0) lbib_fluid_step<T, 0><<<grid, block, 0, d->fluid_stream>>>(p, (const int2*)d->rows);
+  else lbib_fluid_step<T, 1><<<grid, block, 0, d->fluid_stream>>>(p, (const int2*)d->rows);
   d->kernel_launches++;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

@@ -170,14 +170,16 @@ int launch_words(lbib_device* d, const FluidParamsT<T>& p) {
   const unsigned blocks = (unsigned)((threads + WTPB - 1) / WTPB);
   const int zb = 2 + nrz, c = d->cur;
   const unsigned fblocks = (unsigned)sm_count() * 8;
+  /* box mode: the forced cells are among the box's, stepped after the spread */
+  const bool forced = !p.box;
   if (d->parity == 0) {
-    lbib_fluid_step_words<T, V, 0, MINB><<<blocks, WTPB, 0, d->stream>>>(b);
-    lbib_forced_cells<T, 0><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
+    lbib_fluid_step_words<T, V, 0, MINB><<<blocks, WTPB, 0, d->fluid_stream>>>(b);
+    if (forced) lbib_forced_cells<T, 0><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
   } else {
-    lbib_fluid_step_words<T, V, 1, MINB><<<blocks, WTPB, 0, d->stream>>>(b);
-    lbib_forced_cells<T, 1><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
+    lbib_fluid_step_words<T, V, 1, MINB><<<blocks, WTPB, 0, d->fluid_stream>>>(b);
+    if (forced) lbib_forced_cells<T, 1><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
   }
-  d->kernel_launches += 2;
+  d->kernel_launches += forced ? 2 : 1;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -206,20 +208,28 @@ int launch_words_tma(lbib_device* d, const FluidParamsT<T>& p) {
   const unsigned blocks = (unsigned)(g.nitems < cap ? g.nitems : cap);
   const int zb = 2 + nrz, c = d->cur;
   const unsigned fblocks = (unsigned)sm_count() * 8;
+  const bool forced = !p.box;
   if (d->parity == 0) {
-    lbib_fluid_step_words_tma<T, 0, STAGES, MINB><<<blocks, WTPB, smem, d->stream>>>(b, g, d->err);
-    lbib_forced_cells<T, 0><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
+    lbib_fluid_step_words_tma<T, 0, STAGES, MINB><<<blocks, WTPB, smem, d->fluid_stream>>>(b, g, d->err);
+    if (forced) lbib_forced_cells<T, 0><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
   } else {
-    lbib_fluid_step_words_tma<T, 1, STAGES, MINB><<<blocks, WTPB, smem, d->stream>>>(b, g, d->err);
-    lbib_forced_cells<T, 1><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
+    lbib_fluid_step_words_tma<T, 1, STAGES, MINB><<<blocks, WTPB, smem, d->fluid_stream>>>(b, g, d->err);
+    if (forced) lbib_forced_cells<T, 1><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
   }
-  d->kernel_launches += 2;
+  d->kernel_launches += forced ? 2 : 1;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 /* One-grid variants beyond the word-kernel ones of lbib_words.cuh (16-bit
  * storage): {stages, resident CTAs per SM} of the TMA-staged kernel. */
 constexpr int kTmaVariants = 3;
+
+/* The box's cells of a box-mode step (after the spread). */
+template <typename T>
+int lp_box(lbib_device* d) {
+  FluidParamsT<T> p = make_params_t<T>(d, d->steps == 0);
+  return launch_box_cells_t<T>(d, p);
+}
 
 template <typename T>
 int lp_step(lbib_device* d) {
@@ -243,6 +253,15 @@ extern "C" int lbdev_lp_fluid_step(lbib_device* d) {
     case LBIB_PREC_F32: return lp_step<float>(d);
     case LBIB_PREC_F16: return lp_step<__half>(d);
     case LBIB_PREC_BF16: return lp_step<__nv_bfloat16>(d);
+    default: return -1;
+  }
+}
+
+extern "C" int lbdev_lp_box_cells(lbib_device* d) {
+  switch (LBIB_PREC_TYPE(d->prec)) {
+    case LBIB_PREC_F32: return lp_box<float>(d);
+    case LBIB_PREC_F16: return lp_box<__half>(d);
+    case LBIB_PREC_BF16: return lp_box<__nv_bfloat16>(d);
     default: return -1;
   }
 }

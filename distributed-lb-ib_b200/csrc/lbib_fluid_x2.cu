@@ -81,8 +81,8 @@ extern "C" int lbdev_launch_fluid_bulk(lbib_device* d, const void* fluid_params)
     b.pf = (long)d->l2_pf * sms * (d->parity ? LBIB_X2_MINB1 : LBIB_X2_MINB0);
   }
   dim3 grid((unsigned)((long)b.nry * nrz), (unsigned)((b.npairs + TPB - 1) / TPB));
-  if (d->parity == 0) lbib_fluid_step_x2<0><<<grid, TPB, 0, d->stream>>>(b);
-  else lbib_fluid_step_x2<1><<<grid, TPB, 0, d->stream>>>(b);
+  if (d->parity == 0) lbib_fluid_step_x2<0><<<grid, TPB, 0, d->fluid_stream>>>(b);
+  else lbib_fluid_step_x2<1><<<grid, TPB, 0, d->fluid_stream>>>(b);
   d->kernel_launches++;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

@@ -18,21 +18,25 @@ __global__ void lbib_fiber_forces(double* __restrict__ nodes, int R, int C, doub
   fiber_forces_node(nodes, R, C, bc, sc, sc2, ds1, ds2, bend_bug, i);
 }
 
-__global__ void lbib_node_prep(const double* __restrict__ nodes, long S, int nx, int ny, int nz, int ntx, int nty,
-                               double* __restrict__ W, int* __restrict__ st, int* __restrict__ tile_cnt,
-                               int* __restrict__ chunk_box, int* err, int step) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+/* A block per 32-node chunk: warp p evaluates part p of the chunk's nodes
+ * (node_prep_part); warp 0 also reduces the chunk's stencil box. */
+__global__ void __launch_bounds__(128) lbib_node_prep(const double* __restrict__ nodes, long S, int nx, int ny, int nz,
+                                                      int ntx, int nty, double* __restrict__ W, int* __restrict__ st,
+                                                      int* __restrict__ tile_cnt, int* __restrict__ chunk_box, int* err,
+                                                      int step) {
+  const long i = (long)blockIdx.x * 32 + (threadIdx.x & 31);
+  const int part = threadIdx.x >> 5;
   int b0 = INT_MAX, b1 = INT_MIN, b2 = INT_MAX, b3 = INT_MIN, b4 = INT_MAX, b5 = INT_MIN;
-  if (i < S) node_prep_one(nodes, i, nx, ny, nz, ntx, nty, 0, W, st, tile_cnt, err, step, b0, b1, b2, b3, b4, b5);
-  chunk_box_reduce(i, S, chunk_box, b0, b1, b2, b3, b4, b5);
+  if (i < S) node_prep_part(nodes, i, part, nx, ny, nz, ntx, nty, W, st, tile_cnt, err, step, b0, b1, b2, b3, b4, b5);
+  if (part == 0) chunk_box_reduce(i, S, chunk_box, b0, b1, b2, b3, b4, b5);
 }
 
 __global__ void lbib_pair_scatter(const int* __restrict__ st, long S, int ntx, int nty, int nx, int ny, int nz,
                                   const int* __restrict__ slot, const int* __restrict__ slot_off,
                                   int* __restrict__ slot_cursor, int* __restrict__ pair_node, const int* err) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= S || *(volatile const int*)err) return;
-  pair_scatter_one(st, i, ntx, nty, nx, ny, nz, slot, slot_off, slot_cursor, pair_node);
+  if (*(volatile const int*)err) return;   /* uniform: the whole warp returns */
+  pair_scatter_warp(st, i, S, ntx, nty, nx, ny, nz, slot, slot_off, slot_cursor, pair_node);
 }
 
 __global__ void __launch_bounds__(64) lbib_spread_gather(const double* __restrict__ nodes, const double* __restrict__ W,
@@ -61,14 +65,96 @@ __global__ void __launch_bounds__(64) lbib_spread_gather_scan(const double* __re
   }
 }
 
-/* Nodes [i0, i1) of the concatenated sheets. */
-__global__ void lbib_move_nodes(double* __restrict__ nodes, const double* __restrict__ W, const int* __restrict__ st,
-                                long i0, long i1, int ntx, int nty, const int* __restrict__ slot,
-                                const double* __restrict__ Utile, double dt, const int* err) {
+/* Nodes [i0, i1) of the concatenated sheets.  With `box` (an overlapped
+ * step's next box), the box in tiles of the moved nodes' stencils is
+ * reduced into it (block reduction, then six atomics per block). */
+__global__ void __launch_bounds__(128) lbib_move_nodes(double* __restrict__ nodes, const double* __restrict__ W,
+                                                       const int* __restrict__ st, long i0, long i1, int ntx, int nty,
+                                                       const int* __restrict__ slot, const double* __restrict__ Utile,
+                                                       double dt, const int* err, int* __restrict__ box, int nx,
+                                                       int ny, int nz) {
   const long i = i0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1) return;
-  if (*(volatile const int*)err) return;
-  move_node(nodes, W, st, i, ntx, nty, slot, Utile, dt);
+  const bool live = i < i1 && !*(volatile const int*)err;
+  if (live) move_node(nodes, W, st, i, ntx, nty, slot, Utile, dt);
+  if (!box) return;
+  int b[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN};
+  if (live) {
+    const double* m = nodes + i * 12;
+    if (stencil_inside(m[0], nx) && stencil_inside(m[1], ny) && stencil_inside(m[2], nz)) {
+      const int is = stencil_start(m[0]), js = stencil_start(m[1]), ks = stencil_start(m[2]);
+      b[0] = is >> 2; b[1] = (is + 3) >> 2; b[2] = js >> 2; b[3] = (js + 3) >> 2; b[4] = ks >> 2; b[5] = (ks + 3) >> 2;
+    }
+  }
+  __shared__ int red[6][4];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    int v = b[k];
+    for (int o = 16; o > 0; o >>= 1) {
+      const int u = __shfl_xor_sync(0xffffffffu, v, o);
+      v = (k & 1) ? max(v, u) : min(v, u);
+    }
+    if (lane == 0) red[k][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int k = threadIdx.x;
+    int v = red[k][0];
+    for (int j = 1; j < (int)(blockDim.x >> 5); ++j) v = (k & 1) ? max(v, red[k][j]) : min(v, red[k][j]);
+    if ((k & 1) ? v != INT_MIN : v != INT_MAX) {
+      if (k & 1) atomicMax(&box[k], v);
+      else atomicMin(&box[k], v);
+    }
+  }
+}
+
+/* The box, in tiles, of all stencils of the current node positions (one
+ * block): what an overlapped fluid step leaves to the cells kernel that
+ * runs after the spread.  Nodes whose stencil leaves the grid are left out
+ * (the spread reports them).  No valid node: an empty box. */
+__global__ void __launch_bounds__(1024) lbib_stencil_box(const double* __restrict__ nodes, long S, int nx, int ny,
+                                                         int nz, int* __restrict__ box) {
+  __shared__ int red[6][32];
+  int b0 = INT_MAX, b1 = INT_MIN, b2 = INT_MAX, b3 = INT_MIN, b4 = INT_MAX, b5 = INT_MIN;
+  for (long i0 = threadIdx.x; i0 < S; i0 += 4L * blockDim.x) {
+    double x[4][3];   /* four nodes' loads in flight before any is used */
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const long i = i0 + (long)u * blockDim.x;
+      const double* m = nodes + (i < S ? i : 0) * 12;
+      x[u][0] = i < S ? m[0] : -1.0; x[u][1] = m[1]; x[u][2] = m[2];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (!(stencil_inside(x[u][0], nx) && stencil_inside(x[u][1], ny) && stencil_inside(x[u][2], nz))) continue;
+      const int is = stencil_start(x[u][0]), js = stencil_start(x[u][1]), ks = stencil_start(x[u][2]);
+      b0 = min(b0, is); b1 = max(b1, is + 3);
+      b2 = min(b2, js); b3 = max(b3, js + 3);
+      b4 = min(b4, ks); b5 = max(b5, ks + 3);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    b0 = min(b0, __shfl_xor_sync(0xffffffffu, b0, o)); b1 = max(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+    b2 = min(b2, __shfl_xor_sync(0xffffffffu, b2, o)); b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, o));
+    b4 = min(b4, __shfl_xor_sync(0xffffffffu, b4, o)); b5 = max(b5, __shfl_xor_sync(0xffffffffu, b5, o));
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  if (lane == 0) { red[0][w] = b0; red[1][w] = b1; red[2][w] = b2; red[3][w] = b3; red[4][w] = b4; red[5][w] = b5; }
+  __syncthreads();
+  if (w == 0) {
+    b0 = lane < nw ? red[0][lane] : INT_MAX; b1 = lane < nw ? red[1][lane] : INT_MIN;
+    b2 = lane < nw ? red[2][lane] : INT_MAX; b3 = lane < nw ? red[3][lane] : INT_MIN;
+    b4 = lane < nw ? red[4][lane] : INT_MAX; b5 = lane < nw ? red[5][lane] : INT_MIN;
+    for (int o = 16; o > 0; o >>= 1) {
+      b0 = min(b0, __shfl_xor_sync(0xffffffffu, b0, o)); b1 = max(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+      b2 = min(b2, __shfl_xor_sync(0xffffffffu, b2, o)); b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, o));
+      b4 = min(b4, __shfl_xor_sync(0xffffffffu, b4, o)); b5 = max(b5, __shfl_xor_sync(0xffffffffu, b5, o));
+    }
+    if (lane == 0) {
+      if (b0 > b1) { box[0] = 1; box[1] = 0; box[2] = 1; box[3] = 0; box[4] = 1; box[5] = 0; }
+      else { box[0] = b0 >> 2; box[1] = b1 >> 2; box[2] = b2 >> 2; box[3] = b3 >> 2; box[4] = b4 >> 2; box[5] = b5 >> 2; }
+    }
+  }
 }
 
 /* Dense copy of the spread force for getters: zero, then each touched tile. */
@@ -101,15 +187,21 @@ extern "C" int lbdev_launch_fiber_forces(lbib_device* d, int k) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+extern "C" int lbdev_launch_stencil_box(lbib_device* d) {
+  lbib_stencil_box<<<1, 1024, 0, d->stream>>>(d->nodes, d->S, d->nx, d->ny, d->nz, d->box + 6 * d->box_cur);
+  d->kernel_launches++;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
   const int c = d->cur;
   cudaStream_t st = d->stream;
-  if (cudaMemsetAsync(d->tile_cnt, 0, d->ntiles * sizeof(int), st) != cudaSuccess) return -2;
-  if (cudaMemsetAsync(d->tile_slot[c], 0xff, d->ntiles * sizeof(int), st) != cudaSuccess) return -2;
+  /* tile_cnt is left at zero and tile_slot[c] fully rewritten by the
+     compaction, so the step needs no clearing pass */
   const long S = d->S;
   const unsigned nb = (unsigned)((S + 127) / 128);
-  lbib_node_prep<<<nb, 128, 0, st>>>(d->nodes, S, d->nx, d->ny, d->nz, d->ntx, d->nty, d->W, d->st, d->tile_cnt,
-                                     d->chunk_box, d->err, step);
+  lbib_node_prep<<<(unsigned)d->nchunks, 128, 0, st>>>(d->nodes, S, d->nx, d->ny, d->nz, d->ntx, d->nty, d->W, d->st,
+                                                       d->tile_cnt, d->chunk_box, d->err, step);
   const unsigned nblk = (unsigned)((d->ntiles + kScanBlock - 1) / kScanBlock);
   int* block_tiles = d->scan_tmp;
   int* block_pairs = d->scan_tmp + nblk + 1;
@@ -136,14 +228,15 @@ extern "C" int lbdev_launch_move(lbib_device* d) {
   if (!(d->compat & LBIB_OPT_PIN_ROW0)) {
     const unsigned nb = (unsigned)((d->S + 127) / 128);
     lbib_move_nodes<<<nb, 128, 0, d->stream>>>(d->nodes, d->W, d->st, 0, d->S, d->ntx, d->nty, d->tile_slot[c],
-                                               d->Utile[c], (double)d->dt, d->err);
+                                               d->Utile[c], (double)d->dt, d->err, d->box_next, d->nx, d->ny,
+                                               d->nz);
     d->kernel_launches++;
   } else {
     for (int k = 0; k < d->nsheets; ++k) {
       const long i0 = d->sh[k].offset + d->sh[k].cols, i1 = d->sh[k].offset + (long)d->sh[k].rows * d->sh[k].cols;
       const unsigned nb = (unsigned)((i1 - i0 + 127) / 128);
       lbib_move_nodes<<<nb, 128, 0, d->stream>>>(d->nodes, d->W, d->st, i0, i1, d->ntx, d->nty, d->tile_slot[c],
-                                                 d->Utile[c], (double)d->dt, d->err);
+                                                 d->Utile[c], (double)d->dt, d->err, nullptr, d->nx, d->ny, d->nz);
       d->kernel_launches++;
     }
   }

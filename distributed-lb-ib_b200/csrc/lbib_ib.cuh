@@ -187,6 +187,37 @@ __device__ __forceinline__ void node_prep_one(const double* __restrict__ nodes, 
   }
 }
 
+/* node_prep_one for the one-grid kernel, split over four threads per node:
+ * part p (0..3) evaluates the three delta factors of stencil offset p (one
+ * per axis); part 0 also writes the stencil start, checks the grid and
+ * counts the touched tiles.  The same values as node_prep_one, with the
+ * twelve dependent cosine evaluations of a node spread over four warps. */
+__device__ __forceinline__ void node_prep_part(const double* __restrict__ nodes, long i, int part, int nx, int ny,
+                                               int nz, int ntx, int nty, double* __restrict__ W,
+                                               int* __restrict__ st, int* __restrict__ tile_cnt, int* err, int step,
+                                               int& b0, int& b1, int& b2, int& b3, int& b4, int& b5) {
+  const double* m = nodes + i * 12;
+  const bool inside = stencil_inside(m[0], nx) && stencil_inside(m[1], ny) && stencil_inside(m[2], nz);
+  const int is = inside ? stencil_start(m[0]) : 0, js = inside ? stencil_start(m[1]) : 0,
+            ks = inside ? stencil_start(m[2]) : 0;
+  const double cxk = kPi / (2.0 * 1.0);
+  double* w = W + i * 12;
+  w[part] = 1.0e0 + lbib_cos(cxk * (1.0 * (is + part) - m[0]));
+  w[4 + part] = 1.0e0 + lbib_cos(cxk * (1.0 * (js + part) - m[1]));
+  w[8 + part] = 1.0e0 + lbib_cos(cxk * (1.0 * (ks + part) - m[2]));
+  if (part != 0) return;
+  st[i * 3 + 0] = is; st[i * 3 + 1] = js; st[i * 3 + 2] = ks;
+  if (!inside) {
+    set_error(err, -3, step);
+  } else {
+    for (int tz = ks >> 2; tz <= (ks + 3) >> 2; ++tz)
+      for (int ty = js >> 2; ty <= (js + 3) >> 2; ++ty)
+        for (int tx = is >> 2; tx <= (is + 3) >> 2; ++tx)
+          atomicAdd(&tile_cnt[((long)tz * nty + ty) * ntx + tx], 1);
+    b0 = is; b1 = is + 3; b2 = js; b3 = js + 3; b4 = ks; b5 = ks + 3;
+  }
+}
+
 /* The bounding box of a warp's stencils, written by lane 0 for chunk i >> 5. */
 __device__ __forceinline__ void chunk_box_reduce(long i, long S, int* __restrict__ chunk_box, int b0, int b1, int b2,
                                                  int b3, int b4, int b5) {
@@ -262,7 +293,7 @@ static __global__ void lbib_compact_scan(int* __restrict__ block_tiles, int* __r
   block_exclusive_scan(block_pairs, nblocks, nullptr);
 }
 
-static __global__ void lbib_compact_write(const int* __restrict__ cnt, long n, const int* __restrict__ block_tiles,
+static __global__ void lbib_compact_write(int* __restrict__ cnt, long n, const int* __restrict__ block_tiles,
                                    const int* __restrict__ block_pairs, int* __restrict__ list,
                                    int* __restrict__ slot, int* __restrict__ slot_off, int* __restrict__ slot_len,
                                    int* __restrict__ slot_cursor) {
@@ -298,7 +329,10 @@ static __global__ void lbib_compact_write(const int* __restrict__ cnt, long n, c
     slot_off[pos] = block_pairs[blockIdx.x] + sw[warp] + iw - c;
     slot_len[pos] = c;
     slot_cursor[pos] = 0;
+  } else if (i < n) {
+    slot[i] = -1;     /* the whole map is written: no clearing pass before the step */
   }
+  if (i < n && c) cnt[i] = 0;   /* counts start the next step at zero */
 }
 
 /* Every node appends its index to the list of each tile its stencil touches
@@ -315,6 +349,40 @@ __device__ __forceinline__ void pair_scatter_one(const int* __restrict__ st, lon
         const int k = atomicAdd(&slot_cursor[s], 1);
         pair_node[slot_off[s] + k] = (int)i;
       }
+}
+
+/* The same for the one-grid spread, with the atomics aggregated per warp:
+ * the nodes of a warp (consecutive along a fiber) mostly touch the same
+ * tiles, so the lanes that share a slot take their places with one atomic
+ * (the lowest lane adds the group's size, each lane its rank in the group).
+ * The eight tile offsets are walked by every lane, inactive ones included,
+ * so that the warp's lanes meet at each step.  A list's order still depends
+ * on timing; the gather sorts it. */
+__device__ __forceinline__ void pair_scatter_warp(const int* __restrict__ st, long i, long S, int ntx, int nty,
+                                                  int nx, int ny, int nz, const int* __restrict__ slot,
+                                                  const int* __restrict__ slot_off, int* __restrict__ slot_cursor,
+                                                  int* __restrict__ pair_node) {
+  const int lane = threadIdx.x & 31;
+  int is = 0, js = 0, ks = 0;
+  bool ok = i < S;
+  if (ok) {
+    is = st[i * 3 + 0]; js = st[i * 3 + 1]; ks = st[i * 3 + 2];
+    ok = !(is < 0 || is + 3 >= nx || js < 0 || js + 3 >= ny || ks < 0 || ks + 3 >= nz);
+  }
+#pragma unroll
+  for (int o = 0; o < 8; ++o) {
+    const int tx = (is >> 2) + (o & 1), ty = (js >> 2) + ((o >> 1) & 1), tz = (ks >> 2) + (o >> 2);
+    const bool here = ok && tx <= (is + 3) >> 2 && ty <= (js + 3) >> 2 && tz <= (ks + 3) >> 2;
+    const int s = here ? slot[((long)tz * nty + ty) * ntx + tx] : -1;
+    const unsigned grp = __match_any_sync(0xffffffffu, s);
+    if (!here) continue;
+    const int leader = __ffs(grp) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&slot_cursor[s], __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    const int k = base + __popc(grp & ((1u << lane) - 1u));
+    pair_node[slot_off[s] + k] = (int)i;
+  }
 }
 
 /* Longest per-tile node list sorted in shared memory; longer lists take the

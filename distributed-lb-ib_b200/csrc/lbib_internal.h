@@ -133,15 +133,30 @@ typedef struct lbib_device {
   size_t host_reg_bytes[8];
   int nhost_reg;
   cudaStream_t stream;
+  /* the fluid step overlapped with the spread (one-grid steps): the row and
+     bulk kernels run on fluid_stream, skipping the tiles of the box of this
+     step's stencils (box[6], in tiles, computed at the start of the step);
+     the box's cells run on `stream` after the spread */
+  cudaStream_t fluid_stream;     /* == stream unless a step is overlapped     */
+  cudaStream_t side;
+  cudaEvent_t ev_box, ev_bulk;
+  int* box;                      /* [2][6]: this step's box and the next's    */
+  int box_cur;                   /* which of the two this step uses           */
+  int box_valid;                 /* box[box_cur] holds the current positions' */
+  int* box_next;                 /* the move accumulates the next box here    */
+  int box_mode;                  /* 1 inside an overlapped step               */
+  int overlap;                   /* overlapped steps allowed (LBIB_OVERLAP)   */
   int device;
   long kernel_launches;          /* kernels this state has launched           */
   /* optional stage timing: events around the five stages of each step */
   int profiling;
-  cudaEvent_t* prof_ev;          /* [prof_cap][6]                             */
+  cudaEvent_t* prof_ev;          /* [prof_cap][LBIB_PROF_EV]                  */
+  char* prof_overlap;            /* [prof_cap] the step was overlapped        */
   long prof_steps, prof_cap;
 } lbib_device;
 
 #define LBIB_NSTAGE_TIMED 5      /* forces, spread, fluid, moments, move */
+#define LBIB_PROF_EV 9           /* events per profiled step                 */
 
 typedef struct lbdev_config {
   int nx, ny, nz, cube_size, compat, prec;

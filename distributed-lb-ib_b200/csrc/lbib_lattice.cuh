@@ -115,6 +115,12 @@ struct FluidParamsT {
   const int* slot_prev;  /* (rho, u)(t-1) tiles */
   const double* Uprev;
   int ntx, nty;
+  /* box mode (the fluid step overlapped with the spread): the tiles
+     box[0..1] x box[2..3] x box[4..5] (inclusive, in tiles) hold every
+     stencil of this step; the bulk and row kernels skip them and read no
+     force, and a kernel of its own steps their cells after the spread.
+     NULL: the kernels find the forced tiles through slot_cur. */
+  const int* box;
   float sh[19];
   double rhos, uxs;
   /* the same constants in FP32 for the low-precision forms: rho_s, u_s,
@@ -352,6 +358,12 @@ __device__ __forceinline__ void collide(R f[19], R rho, R ux, R uy, R uz, R Fx, 
   relax_pair<FORCED, 13, 14>(f, uy + uz, wr2, r, p);
   relax_pair<FORCED, 15, 16>(f, ux - uy, wr2, r, p);
   relax_pair<FORCED, 17, 18>(f, ux + uy, wr2, r, p);
+}
+
+/* Cell (x, y, z) lies in a tile of the box (box mode). */
+__device__ __forceinline__ bool in_box(const int* box, int x, int y, int z) {
+  const int tx = x >> 2, ty = y >> 2, tz = z >> 2;
+  return tx >= box[0] && tx <= box[1] && ty >= box[2] && ty <= box[3] && tz >= box[4] && tz <= box[5];
 }
 
 __device__ __forceinline__ int tile_of(int x, int y, int z, int ntx, int nty) {

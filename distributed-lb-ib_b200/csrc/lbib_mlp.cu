@@ -1,9 +1,9 @@
 /*
  * A small multilayer perceptron on the GPU -- the surrogate that screens
  * parameter sweeps -- with its training: BF16 weights and activations, FP32
- * accumulation on the tensor cores (warp-level mma.sync m16n8k16 BF16), FP32
- * master weights, GELU hidden layers, a linear output layer, mean-squared
- * error and Adam.  No reference counterpart.
+ * accumulation on the tcgen05 tensor cores, FP32 master weights, GELU
+ * hidden layers, a linear output layer, mean-squared error and Adam.  No
+ * reference counterpart.
  *
  * Shapes: widths w_0 .. w_L (input, hidden..., output); layer l maps w_l to
  * w_{l+1}.  Every width is padded to a multiple of 16 inside (the padded
@@ -13,10 +13,9 @@
  *
  * One GEMM kernel serves all products, C[M][N] = sum_k A(m,k) B(k,n), with
  * A and B read through element strides (so a transposed operand needs no
- * copy): a 64 x 64 tile per 128-thread block, k in slices of 16 staged in
- * shared memory, each warp a 32 x 32 sub-tile of 2 x 4 mma tiles.  The
- * sizes here (batch 1024, width 256) make every GEMM a few microseconds;
- * the training step is bound by its ~20 launches, not by tensor throughput.
+ * copy): tcgen05.mma on 128 x 64 tiles with the accumulator in TMEM
+ * (mlp_gemm_tc below, device helpers in lbib_mlp_tc.cuh), the weight
+ * gradients' long K split four ways with a fixed-order reduction.
  */
 #include <math.h>
 #include <stdint.h>
@@ -31,14 +30,12 @@
 
 namespace {
 
-constexpr int TM = 64, TN = 64, TK = 16;
 
 /* Epilogues of the GEMM. */
 enum Epi {
   EPI_STORE = 0,        /* C (fp32) = acc                                  */
   EPI_BIAS_GELU = 1,    /* Z = acc + b (fp32 out0), A = gelu(Z) (bf16 out1) */
   EPI_BIAS = 2,         /* Y = acc + b (fp32 out0)                          */
-  EPI_GELU_BACK = 3,    /* dZ = acc * gelu'(Z) (bf16 out1), Z in `aux`      */
 };
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
@@ -49,99 +46,18 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return cdf + z * pdf;
 }
 
-__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
 
-/* C[M][N] (row-major, ldc) = A(m,k) B(k,n); A(m,k) = A[m*am + k*ak],
- * B(k,n) = B[k*bk + n*bn]; out-of-range elements read as 0. */
-template <int EPI>
-__global__ void __launch_bounds__(128) mlp_gemm(const __nv_bfloat16* __restrict__ A, long am, long ak,
-                                                const __nv_bfloat16* __restrict__ B, long bk, long bn, int M, int N,
-                                                int K, float* __restrict__ out0, __nv_bfloat16* __restrict__ out1,
-                                                long ldc, const float* __restrict__ bias) {
-  __shared__ __nv_bfloat16 sA[TM][TK + 8];
-  __shared__ __nv_bfloat16 sB[TK][TN + 8];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int g = lane >> 2, t = lane & 3;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
-  const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-  for (int k0 = 0; k0 < K; k0 += TK) {
-    for (int e = tid; e < TM * TK; e += 128) {
-      const int r = e / TK, c = e % TK;
-      const int m = m0 + r, k = k0 + c;
-      sA[r][c] = (m < M && k < K) ? A[m * am + k * ak] : zero;
-    }
-    for (int e = tid; e < TK * TN; e += 128) {
-      const int r = e / TN, c = e % TN;
-      const int k = k0 + r, n = n0 + c;
-      sB[r][c] = (k < K && n < N) ? B[k * bk + n * bn] : zero;
-    }
-    __syncthreads();
-    uint32_t a[2][4], b[4][2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int r = wm + 16 * i + g;
-      a[i][0] = pack2(sA[r][2 * t], sA[r][2 * t + 1]);
-      a[i][1] = pack2(sA[r + 8][2 * t], sA[r + 8][2 * t + 1]);
-      a[i][2] = pack2(sA[r][2 * t + 8], sA[r][2 * t + 9]);
-      a[i][3] = pack2(sA[r + 8][2 * t + 8], sA[r + 8][2 * t + 9]);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int c = wn + 8 * j + g;
-      b[j][0] = pack2(sB[2 * t][c], sB[2 * t + 1][c]);
-      b[j][1] = pack2(sB[2 * t + 8][c], sB[2 * t + 9][c]);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        asm volatile(
-            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-            "{%0,%1,%2,%3};\n"
-            : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-            : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]), "r"(b[j][1]));
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int m = m0 + wm + 16 * i + g + (r >= 2 ? 8 : 0);
-        const int n = n0 + wn + 8 * j + 2 * t + (r & 1);
-        if (m >= M || n >= N) continue;
-        float v = acc[i][j][r];
-        if (EPI == EPI_STORE) {
-          out0[m * ldc + n] = v;
-        } else {
-          v += bias[n];
-          out0[m * ldc + n] = v;
-          if (EPI == EPI_BIAS_GELU) out1[m * ldc + n] = __float2bfloat16(gelu(v));
-        }
-      }
-}
-
-/* The same product and epilogues on the tcgen05 tensor cores (FP32
- * accumulator in TMEM; lbib_mlp_tc.cuh): a 128 x BN tile per 128-thread
- * CTA, K in double-buffered slices of 64.  `err` is set if an mbarrier wait
+/* C[M][N] (row-major, ldc) = A(m,k) B(k,n), A(m,k) = A[m*am + k*ak],
+ * B(k,n) = B[k*bk + n*bn], out-of-range elements read as 0, on the tcgen05
+ * tensor cores (FP32 accumulator in TMEM; lbib_mlp_tc.cuh): a 128 x BN tile
+ * per 128-thread CTA, K in double-buffered slices of 64.  `err` is set if an mbarrier wait
  * ran out (the tile is then not written).
  *
  * Split K (gridDim.z = S > 1, EPI_STORE only): CTA z sums the K slices
  * [z Kc, (z+1) Kc) and writes its partial tile to ws[z]; the CTA that
  * finishes a tile last (a per-tile counter) adds the S partials in z order
  * into out0 and resets the counter -- the same bits whatever the order in
- * which the CTAs run.  `aux` is the bias, or Z for EPI_GELU_BACK. */
+ * which the CTAs run.  `aux` is the bias. */
 constexpr int TC_BN = 64;
 constexpr int kMaxSplit = 8;      /* split-K factors 1, 2, 4, 8             */
 constexpr int kMaxTiles = 4096;   /* output tiles a split GEMM may have     */
@@ -227,8 +143,6 @@ __global__ void __launch_bounds__(lbib_tc::NT) mlp_gemm_tc(const __nv_bfloat16* 
         if (EPI == EPI_STORE) {
           if (S > 1) part[(long)m * ldc + n] = x;
           else out0[(long)m * ldc + n] = x;
-        } else if (EPI == EPI_GELU_BACK) {
-          out1[(long)m * ldc + n] = __float2bfloat16(x * gelu_grad(aux[(long)m * ldc + n]));
         } else {
           x += bias[n];
           out0[(long)m * ldc + n] = x;
@@ -375,7 +289,7 @@ struct lbib_mlp {
   long* wbo;            /* [L] offset of W_l in wbf */
   __nv_bfloat16** act;  /* [L+1] bf16 activations [B][wp_l] (act[0] = input) */
   float** z;            /* [L] pre-activations fp32 [B][wp_{l+1}] */
-  float* dA;            /* fp32 [B][max wp] (the mma.sync path)         */
+  float* dA;            /* fp32 [B][max wp]                               */
   __nv_bfloat16* dZ;    /* bf16 [2][B][max wp]: layer l's dZ, and l-1's  */
   float* ws;            /* split-K partial tiles                          */
   long ws_elems;
@@ -383,7 +297,6 @@ struct lbib_mlp {
   float* part;
   float* d_loss;
   int* d_err;           /* a tensor-core GEMM's mbarrier wait ran out     */
-  int legacy;           /* LBIB_MLP_LEGACY=1: the warp-level mma.sync GEMM */
   int maxw;             /* largest padded width                           */
   long steps;
   cudaStream_t stream;  /* where the work runs: own_stream or the caller's */
@@ -394,56 +307,36 @@ namespace {
 
 int launch_gemm(lbib_mlp* n, int epi, const __nv_bfloat16* A, long am, long ak, const __nv_bfloat16* B, long bk,
                 long bn, int M, int N, int K, float* out0, __nv_bfloat16* out1, long ldc, const float* bias) {
-  if (!n->legacy) {
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(mlp_gemm_tc<EPI_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-      cudaFuncSetAttribute(mlp_gemm_tc<EPI_BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-      cudaFuncSetAttribute(mlp_gemm_tc<EPI_BIAS_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-      cudaFuncSetAttribute(mlp_gemm_tc<EPI_GELU_BACK>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-      attr = true;
-    }
-    dim3 grid((unsigned)((N + TC_BN - 1) / TC_BN), (unsigned)((M + lbib_tc::BM - 1) / lbib_tc::BM), 1);
-    /* a long K over few tiles (the weight gradients, K = batch) is split so
-       that ~32 CTAs share it; the split depends on the shape only */
-    if (epi == EPI_STORE) {
-      const int tiles = (int)(grid.x * grid.y), nkt = (K + lbib_tc::BK - 1) / lbib_tc::BK;
-      int sk = 1;
-      while (sk * 2 <= kMaxSplit && tiles * sk < 32 && nkt >= 4 * sk * 2) sk *= 2;
-      if ((long)sk * M * ldc > n->ws_elems || tiles > kMaxTiles) sk = 1;
-      grid.z = (unsigned)sk;
-    }
-    switch (epi) {
-      case EPI_BIAS_GELU:
-        mlp_gemm_tc<EPI_BIAS_GELU><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0,
-                                                                              out1, ldc, bias, n->d_err, n->ws,
-                                                                              n->tile_cnt);
-        break;
-      case EPI_BIAS:
-        mlp_gemm_tc<EPI_BIAS><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1,
-                                                                         ldc, bias, n->d_err, n->ws, n->tile_cnt);
-        break;
-      case EPI_GELU_BACK:
-        mlp_gemm_tc<EPI_GELU_BACK><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0,
-                                                                              out1, ldc, bias, n->d_err, n->ws,
-                                                                              n->tile_cnt);
-        break;
-      default:
-        mlp_gemm_tc<EPI_STORE><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1,
-                                                                          ldc, bias, n->d_err, n->ws, n->tile_cnt);
-    }
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(mlp_gemm_tc<EPI_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    cudaFuncSetAttribute(mlp_gemm_tc<EPI_BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    cudaFuncSetAttribute(mlp_gemm_tc<EPI_BIAS_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    attr = true;
   }
-  dim3 grid((unsigned)((N + TN - 1) / TN), (unsigned)((M + TM - 1) / TM));
+  dim3 grid((unsigned)((N + TC_BN - 1) / TC_BN), (unsigned)((M + lbib_tc::BM - 1) / lbib_tc::BM), 1);
+  /* a long K over few tiles (the weight gradients, K = batch) is split so
+     that ~32 CTAs share it; the split depends on the shape only */
+  if (epi == EPI_STORE) {
+    const int tiles = (int)(grid.x * grid.y), nkt = (K + lbib_tc::BK - 1) / lbib_tc::BK;
+    int sk = 1;
+    while (sk * 2 <= kMaxSplit && tiles * sk < 32 && nkt >= 4 * sk * 2) sk *= 2;
+    if ((long)sk * M * ldc > n->ws_elems || tiles > kMaxTiles) sk = 1;
+    grid.z = (unsigned)sk;
+  }
   switch (epi) {
     case EPI_BIAS_GELU:
-      mlp_gemm<EPI_BIAS_GELU><<<grid, 128, 0, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1, ldc, bias);
+      mlp_gemm_tc<EPI_BIAS_GELU><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0,
+                                                                            out1, ldc, bias, n->d_err, n->ws,
+                                                                            n->tile_cnt);
       break;
     case EPI_BIAS:
-      mlp_gemm<EPI_BIAS><<<grid, 128, 0, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1, ldc, bias);
+      mlp_gemm_tc<EPI_BIAS><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1,
+                                                                       ldc, bias, n->d_err, n->ws, n->tile_cnt);
       break;
     default:
-      mlp_gemm<EPI_STORE><<<grid, 128, 0, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1, ldc, bias);
+      mlp_gemm_tc<EPI_STORE><<<grid, lbib_tc::NT, TC_SMEM, n->stream>>>(A, am, ak, B, bk, bn, M, N, K, out0, out1,
+                                                                        ldc, bias, n->d_err, n->ws, n->tile_cnt);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
@@ -481,13 +374,12 @@ int backward(lbib_mlp* n, const float* T, int batch) {
     if (l == 0) break;
     /* dZ_{l-1} = (dZ W) * gelu'(Z_{l-1}): M = batch, N = in, K = out */
     const __nv_bfloat16* W = n->wbf + n->wbo[l];
-    if (n->legacy) {
-      if (launch_gemm(n, EPI_STORE, dZ, out, 1, W, in, 1, batch, in, out, n->dA, NULL, in, NULL)) return -2;
-      const long na = (long)batch * in;
-      mlp_gelu_back<<<(unsigned)((na + 255) / 256), 256, 0, n->stream>>>(n->dA, n->z[l - 1], na, dZ_prev);
-    } else if (launch_gemm(n, EPI_GELU_BACK, dZ, out, 1, W, in, 1, batch, in, out, NULL, dZ_prev, in, n->z[l - 1])) {
-      return -2;
-    }
+    /* the GELU derivative (erf and exp per element) is an element-wise
+       kernel of its own: inside the GEMM's epilogue it ran on the GEMM's
+       few CTAs and took longer than the separate launch */
+    if (launch_gemm(n, EPI_STORE, dZ, out, 1, W, in, 1, batch, in, out, n->dA, NULL, in, NULL)) return -2;
+    const long na = (long)batch * in;
+    mlp_gelu_back<<<(unsigned)((na + 255) / 256), 256, 0, n->stream>>>(n->dA, n->z[l - 1], na, dZ_prev);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
@@ -577,10 +469,6 @@ lbib_mlp* lbib_mlp_create(int n_layers, const int* widths, int max_batch, unsign
   }
   n->np = np;
   n->maxw = maxw;
-  {
-    const char* e = getenv("LBIB_MLP_LEGACY");
-    n->legacy = e && e[0] == '1';
-  }
   if (!rc && cudaStreamCreateWithFlags(&n->own_stream, cudaStreamNonBlocking) != cudaSuccess) rc = -2;
   n->stream = n->own_stream;
   const size_t fp = sizeof(float) * np;

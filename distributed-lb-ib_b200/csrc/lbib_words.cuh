@@ -36,6 +36,41 @@ namespace lbib {
 
 constexpr int WTPB = 128;
 
+/* Two FP32 lanes in one 64-bit register, for sm_100's packed FP32
+ * add / sub / mul / fma (each lane rounds as the scalar instruction does):
+ * the word kernel collides two neighbouring cells with one instruction. */
+struct F2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float a, float b) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ F2 f2(float a) { return f2(a, a); }
+__device__ __forceinline__ void split(F2 x, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v)); }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+/* a * b + c */
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
 /* V populations of one plane, V cells apart by one in x, as NR = V S / 4
  * 32-bit registers (S = sizeof(T)); element e sits in register e S / 4,
  * 16-bit elements low half first. */
@@ -168,7 +203,9 @@ struct ItemCtx {
  * here; forced tiles go to lbib_forced_cells. */
 template <typename T, int V>
 __device__ __forceinline__ bool group_here(const WordsParams<T>& b, int g, int y, int z) {
-  return g >= b.g0 && g <= b.g1 && b.p.slot_cur[tile_of(g * V, y, z, b.p.ntx, b.p.nty)] < 0;
+  if (!(g >= b.g0 && g <= b.g1)) return false;
+  if (b.p.box) return !in_box(b.p.box, g * V, y, z);   /* V <= 4: a group is inside one tile */
+  return b.p.slot_cur[tile_of(g * V, y, z, b.p.ntx, b.p.nty)] < 0;
 }
 
 /* t < 2^31 (the launchers check it).  A row's first and last words are
@@ -215,41 +252,6 @@ template <typename T, int V>
 __device__ __forceinline__ const void* edge_src(const typename Word<T, V>::U* src, int dir) {
   if (dir > 0) return sizeof(T) == 2 ? (const void*)(src - 2) : (const void*)(src - 1);
   return (const void*)(src + V);
-}
-
-/* Two FP32 lanes in one 64-bit register, for sm_100's packed FP32
- * add / sub / mul / fma (each lane rounds as the scalar instruction does):
- * the word kernel collides two neighbouring cells with one instruction. */
-struct F2 {
-  unsigned long long v;
-};
-__device__ __forceinline__ F2 f2(float a, float b) {
-  F2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ F2 f2(float a) { return f2(a, a); }
-__device__ __forceinline__ void split(F2 x, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v)); }
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
-  F2 r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
-  F2 r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
-  F2 r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-/* a * b + c */
-__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
-  F2 r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
-  return r;
 }
 
 /* Form<T, true>::moments_free and collide<false> for two cells at once,
@@ -588,6 +590,7 @@ template <typename T, int PAR>
 __device__ __forceinline__ void edge_cell(const FluidParamsT<T>& p, int nry, int r, int k) {
   const int y = 3 + r % nry, z = 3 + r / nry;
   const int x = k < 2 ? 2 + k : p.nx - 6 + k;
+  if (p.box && in_box(p.box, x, y, z)) return;
   step_cell<T, PAR>(p, x, y, z);
 }
 

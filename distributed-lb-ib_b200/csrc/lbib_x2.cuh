@@ -49,7 +49,7 @@ __device__ __forceinline__ void x2_relax_cell(const FluidParams& p, int x, int y
       moments(f, 0.0, 0.0, 0.0, p.half_dt, p.g, rho, ux, uy, uz);
     }
   }
-  const int sc = p.slot_cur[tile];
+  const int sc = p.box ? -1 : p.slot_cur[tile];   /* box mode: only unforced cells get here */
   if (sc >= 0) {
     const double* Ft = p.Fcur + (long)sc * 192;
     collide<true>(f, rho, ux, uy, uz, Ft[cell], Ft[64 + cell], Ft[128 + cell], p);
@@ -67,6 +67,7 @@ __device__ __forceinline__ void x2_load_one(const FluidParams& p, int x, int y, 
 /* The step of the pair (x, x+1) of row (y, z); x even. */
 template <int PAR>
 __device__ __forceinline__ void x2_pair(const FluidParams& p, int x, int y, int z) {
+  if (p.box && in_box(p.box, x, y, z)) return;    /* both cells share a tile (x even) */
   const long idx = sidx(p, x, y, z);
   const long N = p.N, sy = p.sx, sz = (long)p.sx * p.ny;
   const bool pa = (x == 2), pb = (x + 1 == p.nx - 3);
