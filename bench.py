@@ -100,9 +100,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per fused-step launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "lbib_fluid_step_c1.md")
+def profile_traffic(precision="f64"):
+    """DRAM bytes per fused-step launch from the committed ncu summary of the
+    fluid kernel of this storage precision (the FP64 two-cell kernel, or the
+    16-bit word kernel), if any."""
+    name = {"f64": "lbib_fluid_step_c1.md", "f16": "lbib_fluid_step_words_f16_c1.md"}.get(precision.split("-")[0])
+    if name is None:
+        return None
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -395,7 +400,7 @@ def run_lbib(args):
     fluid_ms = stage_ms["fluid"] / max(nprof, 1)
     achieved = bytes_launch / (fluid_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profile_traffic()
+    traffic = profile_traffic(args.precision)
 
     # ---- the FP16-store form of the same workload, same step count
     lp = None
@@ -470,7 +475,8 @@ def run_lbib(args):
                 "config": config_block(args),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                             "kernel": "lbib_fluid_step (fused D3Q19 AA step)",
+                             "kernel": ("lbib_fluid_step (fused D3Q19 AA step)" if args.precision == "f64" else
+                                        "lbib_fluid_step_words (fused D3Q19 AA step, 16-bit words)"),
                              "bytes_per_launch": bytes_launch, "launch_ms": fluid_ms},
                 "stages_ms_per_step": {k: v / max(nprof, 1) for k, v in stage_ms.items()},
                 "gpu_launches": launches, "autotune": tuned, "fp16_store": lp,
@@ -654,7 +660,8 @@ def run_lp_form(args, case, ref_solver, group, value64, peak):
             "speedup_vs_f64": v / value64,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "bytes_per_launch": fluid_cells * 19 * 2 * pop,
-                         "launch_ms": fluid_ms},
+                         "launch_ms": fluid_ms, "traffic": profile_traffic(args.lp_form),
+                         "kernel": "lbib_fluid_step_words (fused D3Q19 AA step, 16-bit words)"},
             "stages_ms_per_step": {k: x / max(nprof, 1) for k, x in stage_ms.items()},
             "autotune": {"variant": best, "ms_per_step": ms_v},
             "error_vs_f64": {"steps": args.warmup + args.steps, "velocity_rel_l2": vel,

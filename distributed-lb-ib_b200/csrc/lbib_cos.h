@@ -121,4 +121,86 @@ LBIB_HD double lbib_cos(double x) {
   return (q == 1 || q == 2) ? -v : v;
 }
 
+/* The same correctly rounded cosine in two phases (Ziv, "Fast evaluation of
+ * elementary mathematical functions with correctly rounded last bit", ACM
+ * TOMS 17(3), 1991; the quick/accurate split of CRlibm, Daramy-Loirat et
+ * al., 2006).  Quick phase: the same reduction, then the series with its
+ * first terms in double-double and its tail from the (2n)! / (2n+1)! term
+ * n = 5 on in plain double, evaluated at z = r^2:
+ *   cos r = 1 + z (c1 + z (c2 + z (c3 + z (c4 + z T(z))))),
+ *   sin r = r (1 + z (s1 + z (s2 + z (s3 + z (s4 + z T'(z)))))).
+ * For |r| <= pi/4 + 2^-50 (z <= 0.62): the tail term z^5 T is below 2^-25
+ * and carries a relative error below 2^-48 from its seven double Horner
+ * steps (alternating, fast-decreasing terms), i.e. below 2^-73 of the
+ * result; the series truncated after n = 11 misses less than 2^-86; the
+ * double-double steps, the reduction and z add less than 2^-98.  The
+ * result (hi, lo) is thus within E < 2^-72 |hi| of the exact value.
+ * Rounding test: with e = 2^-67 |hi| (> 2E plus the rounding of lo -/+ e),
+ * hi + (lo - e) <= exact <= hi + (lo + e), and rounding is monotone, so if
+ * both ends round to the same double that double is the correctly rounded
+ * cosine.  Otherwise (about 1 evaluation in 6000) the accurate phase
+ * lbib_cos decides.  Both phases return the correctly rounded value, so
+ * this function and lbib_cos agree on every argument; the quick phase costs
+ * about a fifth of lbib_cos's FP64 operations. */
+LBIB_HD lbib_dd lbib_dd_mul_d(lbib_dd a, double b) {
+  double p = a.hi * b;
+  double e = fma(a.hi, b, -p);
+  e += a.lo * b;
+  return lbib_quick_two_sum(p, e);
+}
+
+/* The quick phase: 1 and the correctly rounded cosine in *out when the
+ * rounding test decides, 0 otherwise. */
+LBIB_HD int lbib_cos_quick(double x, double* out) {
+  /* (-1)^n / (2n)!  and  (-1)^n / (2n+1)!: n = 1..4 as double-doubles,
+     n = 5..11 as doubles */
+  const double C1 = -0.5, C2H = 0.041666666666666664, C2L = 2.3129646346357427e-18,
+               C3H = -0.001388888888888889, C3L = 5.300543954373577e-20, C4H = 2.48015873015873e-05,
+               C4L = 2.1511947866775882e-23;
+  const double S1H = -0.16666666666666666, S1L = -9.25185853854297e-18, S2H = 0.008333333333333333,
+               S2L = 1.1564823173178714e-19, S3H = -0.0001984126984126984, S3L = -1.7209558293420705e-22,
+               S4H = 2.7557319223985893e-06, S4L = -1.858393274046472e-22;
+  const double CT[7] = {-2.755731922398589e-07, 2.08767569878681e-09, -1.1470745597729725e-11,
+                        4.779477332387385e-14, -1.5619206968586225e-16, 4.110317623312165e-19,
+                        -8.896791392450574e-22};
+  const double ST[7] = {-2.505210838544172e-08, 1.6059043836821613e-10, -7.647163731819816e-13,
+                        2.8114572543455206e-15, -8.22063524662433e-18, 1.9572941063391263e-20,
+                        -3.868170170630684e-23};
+  double kd = rint(x * 0.6366197723675814);
+  int k = (int)kd;
+  lbib_dd r = lbib_two_sum(x, -kd * LBIB_PIO2_1);
+  lbib_dd t2 = {-kd * LBIB_PIO2_2, 0.0};
+  r = lbib_dd_add(r, t2);
+  lbib_dd t3 = {-kd * LBIB_PIO2_3, 0.0};
+  r = lbib_dd_add(r, t3);
+  lbib_dd z = lbib_dd_mul(r, r);
+  int odd = k & 1;
+  const double* T = odd ? ST : CT;
+  double t = T[6];
+  for (int n = 5; n >= 0; --n) t = T[n] + z.hi * t;
+  lbib_dd acc = lbib_dd_mul_d(z, t);
+  lbib_dd c4 = {odd ? S4H : C4H, odd ? S4L : C4L};
+  acc = lbib_dd_add(c4, acc);
+  lbib_dd c3 = {odd ? S3H : C3H, odd ? S3L : C3L};
+  acc = lbib_dd_add(c3, lbib_dd_mul(z, acc));
+  lbib_dd c2 = {odd ? S2H : C2H, odd ? S2L : C2L};
+  acc = lbib_dd_add(c2, lbib_dd_mul(z, acc));
+  lbib_dd c1 = {odd ? S1H : C1, odd ? S1L : 0.0};
+  acc = lbib_dd_add(c1, lbib_dd_mul(z, acc));
+  lbib_dd one = {1.0, 0.0};
+  acc = lbib_dd_add(one, lbib_dd_mul(z, acc));
+  if (odd) acc = lbib_dd_mul(acc, r);
+  const double e = fabs(acc.hi) * 6.776263578034403e-21; /* 2^-67 */
+  const double a = acc.hi + (acc.lo - e), b = acc.hi + (acc.lo + e);
+  if (a != b) return 0;
+  int q = k & 3;
+  *out = (q == 1 || q == 2) ? -a : a;
+  return 1;
+}
+
+LBIB_HD double lbib_cos_2phase(double x) {
+  double v;
+  return lbib_cos_quick(x, &v) ? v : lbib_cos(x);
+}
+
 #endif

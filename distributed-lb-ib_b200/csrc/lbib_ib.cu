@@ -31,37 +31,46 @@ __global__ void __launch_bounds__(128) lbib_node_prep(const double* __restrict__
   if (part == 0) chunk_box_reduce(i, S, chunk_box, b0, b1, b2, b3, b4, b5);
 }
 
+/* Tiles of columns tx in [tlo, thi) only: the slot numbering covers every
+ * touched tile (so that the moment tiles of x-slabs line up), but a slab
+ * lists and gathers only the tiles its own fluid cells read. */
 __global__ void lbib_pair_scatter(const int* __restrict__ st, long S, int ntx, int nty, int nx, int ny, int nz,
-                                  const int* __restrict__ slot, const int* __restrict__ slot_off,
+                                  int tlo, int thi, const int* __restrict__ slot, const int* __restrict__ slot_off,
                                   int* __restrict__ slot_cursor, int* __restrict__ pair_node, const int* err) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (*(volatile const int*)err) return;   /* uniform: the whole warp returns */
-  pair_scatter_warp(st, i, S, ntx, nty, nx, ny, nz, slot, slot_off, slot_cursor, pair_node);
+  pair_scatter_warp(st, i, S, ntx, nty, nx, ny, nz, tlo, thi, slot, slot_off, slot_cursor, pair_node);
 }
 
 __global__ void __launch_bounds__(64) lbib_spread_gather(const double* __restrict__ nodes, const double* __restrict__ W,
                                                          const int* __restrict__ st, const int* __restrict__ list,
                                                          const int* __restrict__ count, const int* __restrict__ slot_off,
                                                          const int* __restrict__ slot_len, const int* __restrict__ pair_node,
-                                                         int ntx, int nty, double* __restrict__ Ftile, const int* err) {
+                                                         int ntx, int nty, int tlo, int thi, double* __restrict__ Ftile,
+                                                         const int* err) {
   __shared__ GatherSmem sm;
   if (*(volatile const int*)err) return;
   const int n = *count;
-  for (int it = blockIdx.x; it < n; it += gridDim.x)
-    gather_tile(sm, nodes, W, st, it, list[it], slot_off, slot_len, pair_node, ntx, nty, Ftile);
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const int tile = list[it], tx = tile % ntx;
+    if (tx < tlo || tx >= thi) continue;   /* uniform over the block */
+    gather_tile(sm, nodes, W, st, it, tile, slot_off, slot_len, pair_node, ntx, nty, Ftile);
+  }
 }
 
 __global__ void __launch_bounds__(64) lbib_spread_gather_scan(const double* __restrict__ nodes, const double* __restrict__ W,
                                                               const int* __restrict__ st, const int* __restrict__ chunk_box,
                                                               long S, long nchunks, const int* __restrict__ list,
                                                               const int* __restrict__ count, const int* __restrict__ slot_len,
-                                                              int ntx, int nty, double* __restrict__ Ftile, const int* err) {
+                                                              int ntx, int nty, int tlo, int thi,
+                                                              double* __restrict__ Ftile, const int* err) {
   __shared__ ScanSmem sm;
   if (*(volatile const int*)err) return;
   const int n = *count;
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    if (slot_len[it] <= kListCap) continue;
-    gather_tile_scan(sm, nodes, W, st, chunk_box, S, 0, nchunks, it, list[it], ntx, nty, Ftile);
+    const int tile = list[it], tx = tile % ntx;
+    if (slot_len[it] <= kListCap || tx < tlo || tx >= thi) continue;
+    gather_tile_scan(sm, nodes, W, st, chunk_box, S, 0, nchunks, it, tile, ntx, nty, Ftile);
   }
 }
 
@@ -157,15 +166,17 @@ __global__ void __launch_bounds__(1024) lbib_stencil_box(const double* __restric
   }
 }
 
-/* Dense copy of the spread force for getters: zero, then each touched tile. */
+/* Dense copy of the spread force for getters: zero, then each touched tile
+ * of columns tx in [tlo, thi) (the tiles this state gathered). */
 __global__ void lbib_scatter_force(const int* __restrict__ list, const int* __restrict__ count,
-                                   const double* __restrict__ Ftile, int nx, int ny, int nz, int ntx, int nty,
-                                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+                                   const double* __restrict__ Ftile, int nx, int ny, int nz, int ntx, int nty, int tlo,
+                                   int thi, double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
   const int n = *count;
   const int cell = threadIdx.x;
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
     const int tile = list[it];
     const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+    if (tx < tlo || tx >= thi) continue;
     const int x = tx * 4 + (cell & 3), y = ty * 4 + ((cell >> 2) & 3), z = tz * 4 + (cell >> 4);
     if (x < nx && y < ny && z < nz) {
       const long idx = ((long)z * ny + y) * nx + x;
@@ -209,13 +220,16 @@ extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
   lbib_compact_scan<<<1, kScanBlock, 0, st>>>(block_tiles, block_pairs, (int)nblk, d->tile_count[c]);
   lbib_compact_write<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, block_tiles, block_pairs, d->tile_list[c],
                                                   d->tile_slot[c], d->slot_off, d->slot_len, d->slot_cursor);
-  lbib_pair_scatter<<<nb, 128, 0, st>>>(d->st, S, d->ntx, d->nty, d->nx, d->ny, d->nz, d->tile_slot[c], d->slot_off,
-                                        d->slot_cursor, d->pair_node, d->err);
+  /* an x-slab lists and gathers the tiles of its own columns only */
+  const int tlo = d->x_lo / 4, thi = (d->x_hi + 3) / 4;
+  lbib_pair_scatter<<<nb, 128, 0, st>>>(d->st, S, d->ntx, d->nty, d->nx, d->ny, d->nz, tlo, thi, d->tile_slot[c],
+                                        d->slot_off, d->slot_cursor, d->pair_node, d->err);
   lbib_spread_gather<<<148 * 16, 64, 0, st>>>(d->nodes, d->W, d->st, d->tile_list[c], d->tile_count[c], d->slot_off,
-                                              d->slot_len, d->pair_node, d->ntx, d->nty, d->Ftile[c], d->err);
+                                              d->slot_len, d->pair_node, d->ntx, d->nty, tlo, thi, d->Ftile[c],
+                                              d->err);
   lbib_spread_gather_scan<<<148 * 4, 64, 0, st>>>(d->nodes, d->W, d->st, d->chunk_box, S, d->nchunks,
-                                                  d->tile_list[c], d->tile_count[c], d->slot_len, d->ntx, d->nty,
-                                                  d->Ftile[c], d->err);
+                                                  d->tile_list[c], d->tile_count[c], d->slot_len, d->ntx, d->nty, tlo,
+                                                  thi, d->Ftile[c], d->err);
   d->kernel_launches += 7;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
@@ -246,7 +260,8 @@ extern "C" int lbdev_launch_move(lbib_device* d) {
 extern "C" int lbdev_launch_scatter_force(lbib_device* d, double* fx, double* fy, double* fz) {
   const int c = d->cur;
   lbib_scatter_force<<<148 * 8, 64, 0, d->stream>>>(d->tile_list[c], d->tile_count[c], d->Ftile[c], d->nx, d->ny,
-                                                     d->nz, d->ntx, d->nty, fx, fy, fz);
+                                                     d->nz, d->ntx, d->nty, d->x_lo / 4, (d->x_hi + 3) / 4, fx, fy,
+                                                     fz);
   d->kernel_launches++;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

@@ -171,9 +171,9 @@ __device__ __forceinline__ void node_prep_one(const double* __restrict__ nodes, 
     const double cxk = kPi / (2.0 * 1.0);
     double* w = W + i * 12;
     for (int a = 0; a < 4; ++a) {
-      w[a] = 1.0e0 + lbib_cos(cxk * (1.0 * (is + a) - m[0]));
-      w[4 + a] = 1.0e0 + lbib_cos(cxk * (1.0 * (js + a) - m[1]));
-      w[8 + a] = 1.0e0 + lbib_cos(cxk * (1.0 * (ks + a) - m[2]));
+      w[a] = 1.0e0 + lbib_cos_2phase(cxk * (1.0 * (is + a) - m[0]));
+      w[4 + a] = 1.0e0 + lbib_cos_2phase(cxk * (1.0 * (js + a) - m[1]));
+      w[8 + a] = 1.0e0 + lbib_cos_2phase(cxk * (1.0 * (ks + a) - m[2]));
     }
     if (!inside) {
       set_error(err, -3, step);
@@ -202,9 +202,9 @@ __device__ __forceinline__ void node_prep_part(const double* __restrict__ nodes,
             ks = inside ? stencil_start(m[2]) : 0;
   const double cxk = kPi / (2.0 * 1.0);
   double* w = W + i * 12;
-  w[part] = 1.0e0 + lbib_cos(cxk * (1.0 * (is + part) - m[0]));
-  w[4 + part] = 1.0e0 + lbib_cos(cxk * (1.0 * (js + part) - m[1]));
-  w[8 + part] = 1.0e0 + lbib_cos(cxk * (1.0 * (ks + part) - m[2]));
+  w[part] = 1.0e0 + lbib_cos_2phase(cxk * (1.0 * (is + part) - m[0]));
+  w[4 + part] = 1.0e0 + lbib_cos_2phase(cxk * (1.0 * (js + part) - m[1]));
+  w[8 + part] = 1.0e0 + lbib_cos_2phase(cxk * (1.0 * (ks + part) - m[2]));
   if (part != 0) return;
   st[i * 3 + 0] = is; st[i * 3 + 1] = js; st[i * 3 + 2] = ks;
   if (!inside) {
@@ -351,7 +351,9 @@ __device__ __forceinline__ void pair_scatter_one(const int* __restrict__ st, lon
       }
 }
 
-/* The same for the one-grid spread, with the atomics aggregated per warp:
+/* The same for the one-grid spread, with the atomics aggregated per warp
+ * and only the tiles of columns tx in [tlo, thi) listed (an x-slab gathers
+ * the force of its own columns only; the whole grid passes [0, ntx)):
  * the nodes of a warp (consecutive along a fiber) mostly touch the same
  * tiles, so the lanes that share a slot take their places with one atomic
  * (the lowest lane adds the group's size, each lane its rank in the group).
@@ -359,7 +361,7 @@ __device__ __forceinline__ void pair_scatter_one(const int* __restrict__ st, lon
  * so that the warp's lanes meet at each step.  A list's order still depends
  * on timing; the gather sorts it. */
 __device__ __forceinline__ void pair_scatter_warp(const int* __restrict__ st, long i, long S, int ntx, int nty,
-                                                  int nx, int ny, int nz, const int* __restrict__ slot,
+                                                  int nx, int ny, int nz, int tlo, int thi, const int* __restrict__ slot,
                                                   const int* __restrict__ slot_off, int* __restrict__ slot_cursor,
                                                   int* __restrict__ pair_node) {
   const int lane = threadIdx.x & 31;
@@ -372,7 +374,8 @@ __device__ __forceinline__ void pair_scatter_warp(const int* __restrict__ st, lo
 #pragma unroll
   for (int o = 0; o < 8; ++o) {
     const int tx = (is >> 2) + (o & 1), ty = (js >> 2) + ((o >> 1) & 1), tz = (ks >> 2) + (o >> 2);
-    const bool here = ok && tx <= (is + 3) >> 2 && ty <= (js + 3) >> 2 && tz <= (ks + 3) >> 2;
+    const bool here = ok && tx <= (is + 3) >> 2 && ty <= (js + 3) >> 2 && tz <= (ks + 3) >> 2 && tx >= tlo &&
+                      tx < thi;
     const int s = here ? slot[((long)tz * nty + ty) * ntx + tx] : -1;
     const unsigned grp = __match_any_sync(0xffffffffu, s);
     if (!here) continue;

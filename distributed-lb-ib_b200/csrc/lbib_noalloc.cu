@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(64) na_gather(const double* __restrict__ nodes
           }
           for (int a = 6 * half; a < 6 * half + 6; ++a) {
             const int ax = a >> 2, off = a & 3;
-            s_w[j][a] = 1.0e0 + lbib_cos(cxk * (1.0 * (st[ax] + off) - m[ax]));
+            s_w[j][a] = 1.0e0 + lbib_cos_2phase(cxk * (1.0 * (st[ax] + off) - m[ax]));
           }
         } else if (half == 0) {
           s_st[j][0] = INT_MIN / 2; s_st[j][1] = INT_MIN / 2; s_st[j][2] = INT_MIN / 2;

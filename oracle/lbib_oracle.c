@@ -651,6 +651,28 @@ int orc_time(const orc_state* s) { return s->time; }
 /* The delta kernel's cosine as this build evaluates it (for tests). */
 double orc_cos(double x) { return ORC_COS(x); }
 
+/* The CUDA path's two-phase form of the same cosine, run on the host (for
+ * tests; correctly rounded builds only): out[i] = lbib_cos_2phase(x[i]),
+ * and, when `slow` is given, slow[i] = 1 where the quick phase left x[i] to
+ * the accurate one.  Returns how many it left, or -1 in a build without the
+ * correctly rounded cosine. */
+long orc_cos_2phase(const double* x, long n, double* out, unsigned char* slow) {
+#ifdef ORC_CR_COS
+  long ns = 0;
+  for (long i = 0; i < n; ++i) {
+    double v;
+    const int quick = lbib_cos_quick(x[i], &v);
+    if (!quick) { v = lbib_cos(x[i]); ++ns; }
+    out[i] = v;
+    if (slow) slow[i] = (unsigned char)!quick;
+  }
+  return ns;
+#else
+  (void)x; (void)n; (void)out; (void)slow;
+  return -1;
+#endif
+}
+
 void orc_get_moments(const orc_state* s, double* rho, double* ux, double* uy, double* uz) {
   memcpy(rho, s->rho, s->N * sizeof(double));
   memcpy(ux, s->ux, s->N * sizeof(double));

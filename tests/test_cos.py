@@ -74,3 +74,66 @@ def test_libm_cosine_differs_on_a_small_fraction(oracle_built):
     for x in [1.2231614256588297, 0.47938056872090196]:
         assert not is_correctly_rounded(x, lm(x))
         assert is_correctly_rounded(x, cr(x))
+
+
+def _two_phase():
+    cr = P.Oracle.load(cr_cos=True)
+    f = cr.orc_cos_2phase
+    f.restype = C.c_long
+    f.argtypes = [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p]
+
+    def run(xs):
+        xs = np.ascontiguousarray(xs, dtype=np.float64)
+        out = np.empty_like(xs)
+        slow = np.zeros(len(xs), dtype=np.uint8)
+        ns = f(xs.ctypes.data, len(xs), out.ctypes.data, slow.ctypes.data)
+        assert ns == int(slow.sum())
+        return out, slow.astype(bool)
+    return run
+
+
+def _accurate(xs):
+    cr, _ = _cos_fns()
+    return np.array([cr(float(x)) for x in xs])
+
+
+def test_two_phase_cosine_equals_the_accurate_one(oracle_built):
+    """The CUDA path's two-phase cosine (quick double / double-double phase
+    with a rounding test, accurate phase on failure) returns the same bits
+    as the accurate double-double cosine: both are correctly rounded.  The
+    quick phase decides all but a small fraction of arguments."""
+    run = _two_phase()
+    rng = np.random.default_rng(11)
+    xs = np.concatenate([delta_args(200000, 12), rng.uniform(-4.0, 4.0, 100000),
+                         rng.uniform(-1e-6, 1e-6, 2000),
+                         (PI_T / 2) * np.array([0.0, 1.0, -1.0, 2.0, -2.0, 0.5, -0.5, 1.5, -1.5]),
+                         np.array([math.pi / 2, -math.pi / 2, math.pi, -math.pi, math.pi / 4,
+                                   3 * math.pi / 4, 1.2231614256588297, 0.47938056872090196,
+                                   -2.1501599567293868, 1.7759313193883071])])
+    # arguments next to k pi/4 (the reduction's switch points and the range ends)
+    near = []
+    for m in range(-5, 6):
+        v = m * math.pi / 4
+        for _ in range(20):
+            near += [v, -v]
+            v = math.nextafter(v, math.inf)
+    xs = np.concatenate([xs, np.array(near)])
+    out, slow = run(xs)
+    ref = _accurate(xs)
+    bad = np.nonzero(out.view(np.int64) != ref.view(np.int64))[0]
+    assert bad.size == 0, [(xs[i], out[i], ref[i]) for i in bad[:5]]
+    assert 0 < slow.sum() < 2e-3 * len(xs), slow.sum()
+
+
+def test_two_phase_fallback_cases_are_correctly_rounded(oracle_built):
+    """The arguments the rounding test leaves to the accurate phase are the
+    ones whose cosine lies close to a rounding boundary; among 400k
+    delta-kernel arguments each of them comes out correctly rounded by the
+    60-digit evaluation, as do the quick phase's results on a sample."""
+    run = _two_phase()
+    xs = delta_args(400000, 21)
+    out, slow = run(xs)
+    idx = np.nonzero(slow)[0]
+    assert 0 < idx.size < 400
+    for i in list(idx) + list(range(200)):
+        assert is_correctly_rounded(float(xs[i]), float(out[i])), xs[i]
