@@ -207,6 +207,13 @@ __device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y,
     return;
   }
   const bool yskip = (kind == K_WALL) && p.yskip_z0 >= 0 && (z == p.yskip_z0 || z == p.yskip_z0 + 1);
+  /* Every link's word is loaded first, from an address chosen without a
+     branch (the pulled slot, or the cell's own slot q where the link's
+     source lies outside I -- also where the value is then replaced by
+     zero_pop), so that the 19 loads are in flight together; the rules
+     are applied to the loaded values afterwards. */
+  T raw[19];
+  unsigned in_mask = 0u, zero_mask = 0u;
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
     const int xs = x - cx(q), ys = y - cy(q);
@@ -217,13 +224,17 @@ __device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y,
     const bool yin = ys >= 2 && ys <= p.ny - 3;
     const bool zin = zs >= 2 && zs <= p.nz - 3;
     const bool xin = xs >= 2 && xs <= p.nx - 3;
-    if (xin && yin && zin) {
-      if (PAR == 0) f[q] = Pop<T>::get(F[q * N + idx]);
-      else f[q] = Pop<T>::get(F[opp(q) * N + idx - link_offset(q, sy, sz) + wrap]);
-    } else {
-      const bool zero = !p.first && (kind == K_SEMI || (yskip && !yin && zin));
-      f[q] = zero ? zero_pop(p, q) : bounced(p, q, Pop<T>::get(F[q * N + idx]));
-    }
+    const bool in = xin && yin && zin;
+    const long a = (PAR == 0 || !in) ? q * N + idx : opp(q) * N + idx - link_offset(q, sy, sz) + wrap;
+    raw[q] = F[a];
+    in_mask |= (in ? 1u : 0u) << q;
+    zero_mask |= ((!in && !p.first && (kind == K_SEMI || (yskip && !yin && zin))) ? 1u : 0u) << q;
+  }
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    const typename Pop<T>::R v = Pop<T>::get(raw[q]);
+    if ((in_mask >> q) & 1u) f[q] = v;
+    else f[q] = ((zero_mask >> q) & 1u) ? zero_pop(p, q) : bounced(p, q, v);
   }
 }
 
@@ -252,8 +263,7 @@ __device__ __forceinline__ void store_post(const FluidParamsT<T>& p, int x, int 
     if (p.periodic_z && zt < 2) { zt += p.nz - 4; wrap = (long)(p.nz - 4) * sz; }
     if (p.periodic_z && zt > p.nz - 3) { zt -= p.nz - 4; wrap = -(long)(p.nz - 4) * sz; }
     const bool in = xt >= 2 && xt <= p.nx - 3 && yt >= 2 && yt <= p.ny - 3 && zt >= 2 && zt <= p.nz - 3;
-    if (in) F[q * N + idx + link_offset(q, sy, sz) + wrap] = Pop<T>::put(f[q]);
-    else F[opp(q) * N + idx] = Pop<T>::put(f[q]);
+    F[in ? q * N + idx + link_offset(q, sy, sz) + wrap : opp(q) * N + idx] = Pop<T>::put(f[q]);
   }
 }
 
