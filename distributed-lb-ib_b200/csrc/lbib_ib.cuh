@@ -398,7 +398,28 @@ struct GatherSmem {
   int st[64][3];
   double w[64][12];
   double fe[64][3];
+  unsigned m32[2][64];   /* per node: the cells of warp 0 / warp 1 its stencil covers */
 };
+
+/* The columns [d, d + 3] of a stencil that starts d cells from a tile's
+ * origin, as a 4-bit mask of the tile's columns 0..3 (0 when |d| > 3). */
+__device__ __forceinline__ unsigned span4(int d) {
+  if (d >= 4 || d <= -4) return 0u;
+  return d >= 0 ? (0xFu << d) & 0xFu : 0xFu >> (-d);
+}
+
+/* The 64 cells of a tile (cell = 16 z + 4 y + x) that a stencil starting at
+ * (dx, dy, dz) from the tile's origin covers, as a 64-bit mask. */
+__device__ __forceinline__ unsigned long long stencil_tile_mask(int dx, int dy, int dz) {
+  const unsigned mx = span4(dx), my = span4(dy), mz = span4(dz);
+  unsigned row = 0u;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) row |= ((my >> j) & 1u) ? mx << (4 * j) : 0u;
+  unsigned long long m = 0ull;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) m |= ((mz >> k) & 1u) ? (unsigned long long)row << (16 * k) : 0ull;
+  return m;
+}
 
 /* Slot `it` (local tile `tile` of a grid with ntx x nty tiles per z layer):
  * sort its node list, then each of the 64 threads sums its cell's
@@ -436,20 +457,31 @@ __device__ __forceinline__ void gather_tile(GatherSmem& sm, const double* __rest
         __syncthreads();
       }
     const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
-    const int gx = tx * 4 + (t & 3), gy = ty * 4 + ((t >> 2) & 3), gz = tz * 4 + (t >> 4);
+    const int x0 = tx * 4, y0 = ty * 4, z0 = tz * 4;
+    const int gx = x0 + (t & 3), gy = y0 + ((t >> 2) & 3), gz = z0 + (t >> 4);
+    const int lane = t & 31;
+    const unsigned* mw = sm.m32[t >> 5];
     double Fx = 0.0, Fy = 0.0, Fz = 0.0;
     for (int b0 = 0; b0 < L; b0 += 64) {
       const int nb = min(64, L - b0);
       if (t < nb) {
         const long nd = ids[b0 + t];
-        s_st[t][0] = st[nd * 3 + 0]; s_st[t][1] = st[nd * 3 + 1]; s_st[t][2] = st[nd * 3 + 2];
+        const int sx = st[nd * 3 + 0], sy = st[nd * 3 + 1], sz = st[nd * 3 + 2];
+        s_st[t][0] = sx; s_st[t][1] = sy; s_st[t][2] = sz;
         for (int a = 0; a < 12; ++a) s_w[t][a] = W[nd * 12 + a];
         s_fe[t][0] = nodes[nd * 12 + 9]; s_fe[t][1] = nodes[nd * 12 + 10]; s_fe[t][2] = nodes[nd * 12 + 11];
+        const unsigned long long m = stencil_tile_mask(sx - x0, sy - y0, sz - z0);
+        sm.m32[0][t] = (unsigned)m;
+        sm.m32[1][t] = (unsigned)(m >> 32);
       }
       __syncthreads();
+      /* node j adds to the cells its stencil covers, in node order; a warp
+         skips the nodes that cover none of its 32 cells (a uniform branch) */
       for (int j = 0; j < nb; ++j) {
-        const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
-        if ((unsigned)a < 4u && (unsigned)b < 4u && (unsigned)e < 4u) {
+        const unsigned m = mw[j];
+        if (m == 0u) continue;
+        if ((m >> lane) & 1u) {
+          const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
           const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
           Fx = Fx + s_fe[j][0] * tmp;
           Fy = Fy + s_fe[j][1] * tmp;

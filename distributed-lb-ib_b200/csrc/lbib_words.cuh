@@ -416,33 +416,25 @@ __device__ __forceinline__ void words_shift(Word<T, V>& w, int q, int lane, cons
 }
 
 /* One thread's V cells of the bulk step: thread t of the flattened
- * (bulk row, word) space of b.  Every word (and, at a warp edge, the
- * extra element) is loaded before the first shuffle: a shuffle needs its
- * word in a register, and loads issued after it would wait for it, which
- * serialised the odd step's x-shifted planes behind one another. */
+ * (bulk row, word) space of b. */
 template <typename T, int V, int PAR>
 __device__ __forceinline__ void words_item(const WordsParams<T>& b, long t) {
   using Wd = Word<T, V>;
   const FluidParamsT<T>& p = b.p;
   const int lane = threadIdx.x & 31;
   const ItemCtx c = item_ctx<T, V>(b, t);
-  Wd w[19];
-  uint32_t edge[19];
-#pragma unroll
-  for (int q = 0; q < 19; ++q) {
-    const auto* src = word_src<T, PAR>(p, c, q);
-    if (c.loads) w[q].load(src); else w[q].clear();
-    edge[q] = 0u;
-    if (PAR == 1 && cx(q) != 0) {
-      const bool edge_lane = (cx(q) == 1 ? lane == 0 : lane == 31) && c.active;
-      if (edge_lane) edge[q] = *reinterpret_cast<const uint32_t*>(edge_src<T, V>(src, cx(q)));
-    }
-  }
   float d[19 * V];  /* d[q * V + e]: population q of cell x0 + e */
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
-    if (PAR == 1 && cx(q) != 0) words_shift(w[q], q, lane, c, edge[q]);
-    w[q].unpack(d + q * V, 1);
+    Wd w;
+    const auto* src = word_src<T, PAR>(p, c, q);
+    if (c.loads) w.load(src); else w.clear();
+    if (PAR == 1 && cx(q) != 0) {
+      const bool edge_lane = (cx(q) == 1 ? lane == 0 : lane == 31) && c.active;
+      const uint32_t edge = edge_lane ? *reinterpret_cast<const uint32_t*>(edge_src<T, V>(src, cx(q))) : 0u;
+      words_shift(w, q, lane, c, edge);
+    }
+    w.unpack(d + q * V, 1);
   }
   words_collide_store<T, V, PAR>(p, c, lane, d);
 }
