@@ -595,10 +595,10 @@ def run_surrogate_leg(args):
     import surrogate
     t0 = time.perf_counter()
     r = surrogate.pipeline(train_n=args.sur_train, eval_n=args.sur_eval, steps=3000, every=100,
-                           iters=args.sur_iters, members=3, calib_frac=0.25, target=0.98)
+                           iters=args.sur_iters, members=5, calib_frac=0.25, target=0.99)
     e = r["evaluation"]
     return {"workload": f"learned sweep, 96x48x48 lattice, 32x32 sheet, T=3000: {args.sur_train} training runs "
-                        f"(cut from 4096), {args.sur_eval} held-out points (cut from 2048), MLP 5->4x256->192 x3 "
+                        f"(cut from 4096), {args.sur_eval} held-out points (cut from 2048), MLP 5->4x256->192 x5 "
                         f"members, {args.sur_iters} Adam steps of 1024",
             "unit": "points/s",
             "plain_fp64_points_per_s": e["plain_points_per_s"], "plain_fp64_s": e["plain_fp64_s"],

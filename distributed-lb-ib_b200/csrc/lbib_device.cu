@@ -336,7 +336,7 @@ extern "C" int lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_de
     CK(cudaMalloc(&d->slot_off, sizeof(int) * d->cap));
     CK(cudaMalloc(&d->slot_len, sizeof(int) * d->cap));
     CK(cudaMalloc(&d->slot_cursor, sizeof(int) * d->cap));
-    CK(cudaMalloc(&d->pair_node, sizeof(int) * 8 * S));
+    CK(cudaMalloc(&d->pair_node, sizeof(int2) * 8 * S));
     CK(cudaMalloc(&d->scan_tmp, sizeof(int) * 2 * ((d->ntiles + 1023) / 1024 + 1)));
   }
   free(d->sh);

@@ -36,41 +36,39 @@ __global__ void __launch_bounds__(128) lbib_node_prep(const double* __restrict__
  * lists and gathers only the tiles its own fluid cells read. */
 __global__ void lbib_pair_scatter(const int* __restrict__ st, long S, int ntx, int nty, int nx, int ny, int nz,
                                   int tlo, int thi, const int* __restrict__ slot, const int* __restrict__ slot_off,
-                                  int* __restrict__ slot_cursor, int* __restrict__ pair_node, const int* err) {
+                                  int* __restrict__ slot_cursor, int2* __restrict__ ent, const int* err) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (*(volatile const int*)err) return;   /* uniform: the whole warp returns */
-  pair_scatter_warp(st, i, S, ntx, nty, nx, ny, nz, tlo, thi, slot, slot_off, slot_cursor, pair_node);
+  pair_scatter_warp(st, i, S, ntx, nty, nx, ny, nz, tlo, thi, slot, slot_off, slot_cursor, ent);
 }
 
+/* Every listed tile: from its entries (gather_tile_ent), or, with more
+ * than kListCap nodes (a crumpled sheet), by scanning the node chunks in
+ * order (gather_tile_scan). */
 __global__ void __launch_bounds__(64) lbib_spread_gather(const double* __restrict__ nodes, const double* __restrict__ W,
-                                                         const int* __restrict__ st, const int* __restrict__ list,
+                                                         const int* __restrict__ st, const int* __restrict__ chunk_box,
+                                                         long S, long nchunks, const int* __restrict__ list,
                                                          const int* __restrict__ count, const int* __restrict__ slot_off,
-                                                         const int* __restrict__ slot_len, const int* __restrict__ pair_node,
-                                                         int ntx, int nty, int tlo, int thi, double* __restrict__ Ftile,
-                                                         const int* err) {
-  __shared__ GatherSmem sm;
+                                                         const int* __restrict__ slot_len,
+                                                         const int* __restrict__ slot_cursor,
+                                                         const int2* __restrict__ ent, int ntx, int nty, int tlo,
+                                                         int thi, double* __restrict__ Ftile, const int* err) {
+  __shared__ union {
+    GatherSmemE e;
+    ScanSmem s;
+  } sm;
   if (*(volatile const int*)err) return;
   const int n = *count;
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
     const int tile = list[it], tx = tile % ntx;
     if (tx < tlo || tx >= thi) continue;   /* uniform over the block */
-    gather_tile(sm, nodes, W, st, it, tile, slot_off, slot_len, pair_node, ntx, nty, Ftile);
-  }
-}
-
-__global__ void __launch_bounds__(64) lbib_spread_gather_scan(const double* __restrict__ nodes, const double* __restrict__ W,
-                                                              const int* __restrict__ st, const int* __restrict__ chunk_box,
-                                                              long S, long nchunks, const int* __restrict__ list,
-                                                              const int* __restrict__ count, const int* __restrict__ slot_len,
-                                                              int ntx, int nty, int tlo, int thi,
-                                                              double* __restrict__ Ftile, const int* err) {
-  __shared__ ScanSmem sm;
-  if (*(volatile const int*)err) return;
-  const int n = *count;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int tile = list[it], tx = tile % ntx;
-    if (slot_len[it] <= kListCap || tx < tlo || tx >= thi) continue;
-    gather_tile_scan(sm, nodes, W, st, chunk_box, S, 0, nchunks, it, tile, ntx, nty, Ftile);
+    const int L = slot_len[it];
+    if (L <= kListCap) {
+      gather_tile_ent(sm.e, nodes, W, st, it, tile, L, slot_cursor[it], ent + slot_off[it], ntx, nty, Ftile);
+    } else {
+      __syncthreads();   /* the union's previous contents are no longer read */
+      gather_tile_scan(sm.s, nodes, W, st, chunk_box, S, 0, nchunks, it, tile, ntx, nty, Ftile);
+    }
   }
 }
 
@@ -222,15 +220,13 @@ extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
                                                   d->tile_slot[c], d->slot_off, d->slot_len, d->slot_cursor);
   /* an x-slab lists and gathers the tiles of its own columns only */
   const int tlo = d->x_lo / 4, thi = (d->x_hi + 3) / 4;
+  int2* ent = reinterpret_cast<int2*>(d->pair_node);
   lbib_pair_scatter<<<nb, 128, 0, st>>>(d->st, S, d->ntx, d->nty, d->nx, d->ny, d->nz, tlo, thi, d->tile_slot[c],
-                                        d->slot_off, d->slot_cursor, d->pair_node, d->err);
-  lbib_spread_gather<<<148 * 16, 64, 0, st>>>(d->nodes, d->W, d->st, d->tile_list[c], d->tile_count[c], d->slot_off,
-                                              d->slot_len, d->pair_node, d->ntx, d->nty, tlo, thi, d->Ftile[c],
-                                              d->err);
-  lbib_spread_gather_scan<<<148 * 4, 64, 0, st>>>(d->nodes, d->W, d->st, d->chunk_box, S, d->nchunks,
-                                                  d->tile_list[c], d->tile_count[c], d->slot_len, d->ntx, d->nty, tlo,
-                                                  thi, d->Ftile[c], d->err);
-  d->kernel_launches += 7;
+                                        d->slot_off, d->slot_cursor, ent, d->err);
+  lbib_spread_gather<<<148 * 12, 64, 0, st>>>(d->nodes, d->W, d->st, d->chunk_box, S, d->nchunks, d->tile_list[c],
+                                              d->tile_count[c], d->slot_off, d->slot_len, d->slot_cursor, ent,
+                                              d->ntx, d->nty, tlo, thi, d->Ftile[c], d->err);
+  d->kernel_launches += 6;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

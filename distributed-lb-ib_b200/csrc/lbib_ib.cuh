@@ -351,19 +351,20 @@ __device__ __forceinline__ void pair_scatter_one(const int* __restrict__ st, lon
       }
 }
 
-/* The same for the one-grid spread, with the atomics aggregated per warp
- * and only the tiles of columns tx in [tlo, thi) listed (an x-slab gathers
- * the force of its own columns only; the whole grid passes [0, ntx)):
- * the nodes of a warp (consecutive along a fiber) mostly touch the same
- * tiles, so the lanes that share a slot take their places with one atomic
- * (the lowest lane adds the group's size, each lane its rank in the group).
- * The eight tile offsets are walked by every lane, inactive ones included,
- * so that the warp's lanes meet at each step.  A list's order still depends
- * on timing; the gather sorts it. */
+/* The one-grid spread's lists hold entries instead of node indices: the
+ * nodes of a warp (32 consecutive nodes, chunk i >> 5) that touch a tile
+ * at the same stencil offset append one entry {chunk, lane mask} with one
+ * atomic.  A node touches a tile at one offset only, so the masks a chunk
+ * leaves in one list are disjoint; the gather merges them.  Only the
+ * tiles of columns tx in [tlo, thi) are listed (an x-slab gathers the
+ * force of its own columns only; the whole grid passes [0, ntx)).  The
+ * eight tile offsets are walked by every lane, inactive ones included, so
+ * that the warp's lanes meet at each step.  An entry's place in its list
+ * depends on timing; the gather sorts the entries. */
 __device__ __forceinline__ void pair_scatter_warp(const int* __restrict__ st, long i, long S, int ntx, int nty,
                                                   int nx, int ny, int nz, int tlo, int thi, const int* __restrict__ slot,
                                                   const int* __restrict__ slot_off, int* __restrict__ slot_cursor,
-                                                  int* __restrict__ pair_node) {
+                                                  int2* __restrict__ ent) {
   const int lane = threadIdx.x & 31;
   int is = 0, js = 0, ks = 0;
   bool ok = i < S;
@@ -378,13 +379,9 @@ __device__ __forceinline__ void pair_scatter_warp(const int* __restrict__ st, lo
                       tx < thi;
     const int s = here ? slot[((long)tz * nty + ty) * ntx + tx] : -1;
     const unsigned grp = __match_any_sync(0xffffffffu, s);
-    if (!here) continue;
-    const int leader = __ffs(grp) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(&slot_cursor[s], __popc(grp));
-    base = __shfl_sync(grp, base, leader);
-    const int k = base + __popc(grp & ((1u << lane) - 1u));
-    pair_node[slot_off[s] + k] = (int)i;
+    if (!here || lane != __ffs(grp) - 1) continue;
+    const int k = atomicAdd(&slot_cursor[s], 1);
+    ent[slot_off[s] + k] = make_int2((int)(i >> 5), (int)grp);
   }
 }
 
@@ -493,6 +490,122 @@ __device__ __forceinline__ void gather_tile(GatherSmem& sm, const double* __rest
     double* Ft = Ftile + (long)it * 192;
     Ft[t] = Fx; Ft[64 + t] = Fy; Ft[128 + t] = Fz;
   }
+}
+
+/* Shared memory of one entry-list gather CTA (64 threads = one 4^3 tile):
+ * the list's entries as sort keys (chunk << 32 | lane mask) while the node
+ * list is built, then the staged node data while it is summed. */
+struct GatherSmemE {
+  int ids[kListCap];                 /* the tile's nodes in index order       */
+  int seg[kListCap];                 /* per entry: first node position, or -1 */
+  unsigned m32[2][64];               /* per node: the cells of warp 0 / 1     */
+  union {
+    unsigned long long key[kListCap];
+    struct {
+      int st[64][3];
+      double w[64][12];
+      double fe[64][3];
+    } n;
+  } u;
+};
+
+/* Slot `it` (local tile `tile`) from its E entries {chunk, lane mask}: the
+ * entries are sorted by chunk (bitonic, in shared memory), the masks of a
+ * chunk merged, and the node list written in index order; then each of
+ * the 64 threads sums its cell's contributions in node order -- the
+ * reference's (sheet, row, col) order -- into Ftile[it].  The same values
+ * as gather_tile. */
+__device__ __forceinline__ void gather_tile_ent(GatherSmemE& sm, const double* __restrict__ nodes,
+                                                const double* __restrict__ W, const int* __restrict__ st, int it,
+                                                int tile, int L, int E, const int2* __restrict__ ent,
+                                                int ntx, int nty, double* __restrict__ Ftile) {
+  const int t = threadIdx.x;
+  const double cf = 1.0 / (64.0 * 1.0 * 1.0 * 1.0);
+  unsigned long long* key = sm.u.key;
+  int P = 1;
+  while (P < E) P <<= 1;
+  __syncthreads();   /* the previous tile's data is no longer read */
+  for (int k = t; k < P; k += 64) {
+    unsigned long long v = ~0ull;
+    if (k < E) {
+      const int2 e = ent[k];
+      v = ((unsigned long long)(unsigned)e.x << 32) | (unsigned)e.y;
+    }
+    key[k] = v;
+  }
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int a = t; a < P; a += 64) {
+        const int b = a ^ j;
+        if (b > a) {
+          const unsigned long long va = key[a], vb = key[b];
+          const bool up = (a & k) == 0;
+          if ((va > vb) == up) { key[a] = vb; key[b] = va; }
+        }
+      }
+      __syncthreads();
+    }
+  /* entries of one chunk are now adjacent: the first of each run takes the
+     run's merged mask and its first position (a short serial pass) */
+  if (t == 0) {
+    int pos = 0;
+    for (int e = 0; e < E;) {
+      const unsigned ch = (unsigned)(key[e] >> 32);
+      unsigned m = (unsigned)key[e];
+      int f = e + 1;
+      while (f < E && (unsigned)(key[f] >> 32) == ch) { m |= (unsigned)key[f]; sm.seg[f] = -1; ++f; }
+      key[e] = ((unsigned long long)ch << 32) | m;
+      sm.seg[e] = pos;
+      pos += __popc(m);
+      e = f;
+    }
+  }
+  __syncthreads();
+  for (int e = t; e < E; e += 64) {
+    int pos = sm.seg[e];
+    if (pos < 0) continue;
+    const int base = (int)(key[e] >> 32) * 32;
+    for (unsigned m = (unsigned)key[e]; m; m &= m - 1) sm.ids[pos++] = base + __ffs(m) - 1;
+  }
+  __syncthreads();   /* ids complete; key no longer read (aliases the node data) */
+  auto& s_st = sm.u.n.st;
+  auto& s_w = sm.u.n.w;
+  auto& s_fe = sm.u.n.fe;
+  const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+  const int x0 = tx * 4, y0 = ty * 4, z0 = tz * 4;
+  const int gx = x0 + (t & 3), gy = y0 + ((t >> 2) & 3), gz = z0 + (t >> 4);
+  const int lane = t & 31;
+  const unsigned* mw = sm.m32[t >> 5];
+  double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+  for (int b0 = 0; b0 < L; b0 += 64) {
+    const int nb = min(64, L - b0);
+    if (t < nb) {
+      const long nd = sm.ids[b0 + t];
+      const int sx = st[nd * 3 + 0], sy = st[nd * 3 + 1], sz = st[nd * 3 + 2];
+      s_st[t][0] = sx; s_st[t][1] = sy; s_st[t][2] = sz;
+      for (int a = 0; a < 12; ++a) s_w[t][a] = W[nd * 12 + a];
+      s_fe[t][0] = nodes[nd * 12 + 9]; s_fe[t][1] = nodes[nd * 12 + 10]; s_fe[t][2] = nodes[nd * 12 + 11];
+      const unsigned long long m = stencil_tile_mask(sx - x0, sy - y0, sz - z0);
+      sm.m32[0][t] = (unsigned)m;
+      sm.m32[1][t] = (unsigned)(m >> 32);
+    }
+    __syncthreads();
+    for (int j = 0; j < nb; ++j) {
+      const unsigned m = mw[j];
+      if (m == 0u) continue;
+      if ((m >> lane) & 1u) {
+        const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
+        const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
+        Fx = Fx + s_fe[j][0] * tmp;
+        Fy = Fy + s_fe[j][1] * tmp;
+        Fz = Fz + s_fe[j][2] * tmp;
+      }
+    }
+    __syncthreads();
+  }
+  double* Ft = Ftile + (long)it * 192;
+  Ft[t] = Fx; Ft[64 + t] = Fy; Ft[128 + t] = Fz;
 }
 
 /* Crowded tiles (more than kListCap nodes, e.g. a crumpled sheet): visit the

@@ -105,7 +105,7 @@ typedef struct lbib_device {
   int* slot_off;                 /* [cap] start of the slot's node list       */
   int* slot_len;                 /* [cap] length of the slot's node list      */
   int* slot_cursor;              /* [cap] fill cursor                         */
-  int* pair_node;                /* [8 S] node lists of the touched tiles     */
+  int* pair_node;                /* [8 S] int2 entry lists of the touched tiles */
   int* tile_slot[2];             /* [ntiles] slot or -1                       */
   int* tile_list[2];             /* [cap] touched tiles in index order        */
   int* tile_count[2];            /* [1]                                       */
