@@ -475,6 +475,11 @@ FluidParamsT<T> make_params_t(lbib_device* d, int first) {
     const double a0 = cx(q) * p.uxs;
     p.fC[q] = (float)(p.rhos * (3.0 * a0 + 4.5 * a0 * a0 - 1.5 * p.uxs * p.uxs));
   }
+  const long sy = p.sx, sz = (long)p.sx * p.ny;
+  for (int q = 0; q < 19; ++q) {
+    p.pull[q] = opp(q) * p.N - link_offset(q, sy, sz);
+    p.push[q] = q * p.N + link_offset(q, sy, sz);
+  }
   return p;
 }
 

@@ -130,6 +130,11 @@ struct FluidParamsT {
      the deviation equilibrium) */
   float fitw0, fitw1, fitw2;
   float fC[19];
+  /* element offsets from a cell's slot index for the odd step: the pull of
+     direction q (slot opp(q) of x - c_q) and its push (slot q of x + c_q),
+     precomputed so that a kernel forms each of its 38 addresses with one
+     add */
+  long pull[19], push[19];
 };
 
 /* A bounce-back link delivers this cell's own outgoing population opp(q) as
@@ -163,7 +168,7 @@ __device__ __forceinline__ long sidx(const P& p, int x, int y, int z) {
   return ((long)z * p.ny + y) * p.sx + (x - p.gx0);
 }
 
-__device__ __forceinline__ long link_offset(int q, long sy, long sz) {
+__host__ __device__ __forceinline__ long link_offset(int q, long sy, long sz) {
   return (long)cx(q) + (long)cy(q) * sy + (long)cz(q) * sz;
 }
 
@@ -200,10 +205,7 @@ __device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y,
   const long sy = p.sx, sz = (long)p.sx * p.ny;
   if (kind == K_FAST) {
 #pragma unroll
-    for (int q = 0; q < 19; ++q) {
-      if (PAR == 0) f[q] = Pop<T>::get(F[q * N + idx]);
-      else f[q] = Pop<T>::get(F[opp(q) * N + idx - link_offset(q, sy, sz)]);
-    }
+    for (int q = 0; q < 19; ++q) f[q] = Pop<T>::get(PAR == 0 ? F[q * N + idx] : F[idx + p.pull[q]]);
     return;
   }
   const bool yskip = (kind == K_WALL) && p.yskip_z0 >= 0 && (z == p.yskip_z0 || z == p.yskip_z0 + 1);
@@ -225,7 +227,7 @@ __device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y,
     const bool zin = zs >= 2 && zs <= p.nz - 3;
     const bool xin = xs >= 2 && xs <= p.nx - 3;
     const bool in = xin && yin && zin;
-    const long a = (PAR == 0 || !in) ? q * N + idx : opp(q) * N + idx - link_offset(q, sy, sz) + wrap;
+    const long a = (PAR == 0 || !in) ? q * N + idx : idx + p.pull[q] + wrap;
     raw[q] = F[a];
     in_mask |= (in ? 1u : 0u) << q;
     zero_mask |= ((!in && !p.first && (kind == K_SEMI || (yskip && !yin && zin))) ? 1u : 0u) << q;
@@ -252,7 +254,7 @@ __device__ __forceinline__ void store_post(const FluidParamsT<T>& p, int x, int 
   const long sy = p.sx, sz = (long)p.sx * p.ny;
   if (kind == K_FAST) {
 #pragma unroll
-    for (int q = 0; q < 19; ++q) F[q * N + idx + link_offset(q, sy, sz)] = Pop<T>::put(f[q]);
+    for (int q = 0; q < 19; ++q) F[idx + p.push[q]] = Pop<T>::put(f[q]);
     return;
   }
 #pragma unroll
@@ -263,7 +265,7 @@ __device__ __forceinline__ void store_post(const FluidParamsT<T>& p, int x, int 
     if (p.periodic_z && zt < 2) { zt += p.nz - 4; wrap = (long)(p.nz - 4) * sz; }
     if (p.periodic_z && zt > p.nz - 3) { zt -= p.nz - 4; wrap = -(long)(p.nz - 4) * sz; }
     const bool in = xt >= 2 && xt <= p.nx - 3 && yt >= 2 && yt <= p.ny - 3 && zt >= 2 && zt <= p.nz - 3;
-    F[in ? q * N + idx + link_offset(q, sy, sz) + wrap : opp(q) * N + idx] = Pop<T>::put(f[q]);
+    F[in ? idx + p.push[q] + wrap : opp(q) * N + idx] = Pop<T>::put(f[q]);
   }
 }
 

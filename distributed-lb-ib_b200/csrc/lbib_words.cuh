@@ -242,7 +242,8 @@ __device__ __forceinline__ const typename Word<T, 2>::U* word_src(const FluidPar
   const U* F = reinterpret_cast<const U*>(p.f);
   const long sy = p.nx, sz = (long)p.nx * p.ny;
   if (PAR == 0) return F + q * p.N + c.row + c.x0;
-  return F + opp(q) * p.N + c.row - cy(q) * sy - cz(q) * sz + c.x0;
+  (void)sy; (void)sz;
+  return F + c.row + c.x0 + (p.pull[q] + cx(q));   /* the aligned word; the x shift is done in registers */
 }
 
 /* The 4-byte aligned word that holds the element a lane at a warp edge needs
@@ -367,7 +368,7 @@ __device__ __forceinline__ void words_collide_store(const FluidParamsT<T>& p, co
     if (PAR == 0) {
       if (c.active) w.store(F + opp(q) * N + c.row + c.x0);
     } else {
-      U* dst = F + q * N + c.row + cy(q) * sy + cz(q) * sz + c.x0;
+      U* dst = F + c.row + c.x0 + (p.push[q] - cx(q));   /* the aligned word the push lands in */
       if (cx(q) == 0) {
         if (c.active) w.store(dst);
       } else if (cx(q) == 1) {

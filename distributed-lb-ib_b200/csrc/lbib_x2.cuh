@@ -69,19 +69,19 @@ template <int PAR>
 __device__ __forceinline__ void x2_pair(const FluidParams& p, int x, int y, int z) {
   if (p.box && in_box(p.box, x, y, z)) return;    /* both cells share a tile (x even) */
   const long idx = sidx(p, x, y, z);
-  const long N = p.N, sy = p.sx, sz = (long)p.sx * p.ny;
   const bool pa = (x == 2), pb = (x + 1 == p.nx - 3);
   double* __restrict__ F = p.f;
   double fa[19], fb[19];
+  double* __restrict__ Fi = F + idx;
   if (!pa && !pb) {
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
       if (PAR == 0 || cx(q) == 0) {
-        const double* src = PAR ? F + opp(q) * N + idx - link_offset(q, sy, sz) : F + q * N + idx;
+        const double* src = PAR ? Fi + p.pull[q] : Fi + q * p.N;
         const double2 v = *reinterpret_cast<const double2*>(src);
         fa[q] = v.x; fb[q] = v.y;
       } else {
-        const double* src = F + opp(q) * N + idx - link_offset(q, sy, sz);
+        const double* src = Fi + p.pull[q];
         fa[q] = src[0]; fb[q] = src[1];
       }
     }
@@ -94,11 +94,11 @@ __device__ __forceinline__ void x2_pair(const FluidParams& p, int x, int y, int 
   if (PAR == 0) {
 #pragma unroll
     for (int q = 0; q < 19; ++q)
-      *reinterpret_cast<double2*>(F + opp(q) * N + idx) = make_double2(fa[q], fb[q]);
+      *reinterpret_cast<double2*>(Fi + opp(q) * p.N) = make_double2(fa[q], fb[q]);
   } else if (!pa && !pb) {
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
-      double* dst = F + q * N + idx + link_offset(q, sy, sz);
+      double* dst = Fi + p.push[q];
       if (cx(q) == 0) *reinterpret_cast<double2*>(dst) = make_double2(fa[q], fb[q]);
       else { dst[0] = fa[q]; dst[1] = fb[q]; }
     }
