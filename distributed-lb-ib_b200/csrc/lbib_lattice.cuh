@@ -227,7 +227,7 @@ __device__ __forceinline__ void load_pre(const FluidParamsT<T>& p, int x, int y,
     const bool zin = zs >= 2 && zs <= p.nz - 3;
     const bool xin = xs >= 2 && xs <= p.nx - 3;
     const bool in = xin && yin && zin;
-    const long a = (PAR == 0 || !in) ? q * N + idx : idx + p.pull[q] + wrap;
+    const long a = (PAR == 0 || !in) ? q * N + idx : opp(q) * N + idx - link_offset(q, sy, sz) + wrap;
     raw[q] = F[a];
     in_mask |= (in ? 1u : 0u) << q;
     zero_mask |= ((!in && !p.first && (kind == K_SEMI || (yskip && !yin && zin))) ? 1u : 0u) << q;
@@ -265,7 +265,7 @@ __device__ __forceinline__ void store_post(const FluidParamsT<T>& p, int x, int 
     if (p.periodic_z && zt < 2) { zt += p.nz - 4; wrap = (long)(p.nz - 4) * sz; }
     if (p.periodic_z && zt > p.nz - 3) { zt -= p.nz - 4; wrap = -(long)(p.nz - 4) * sz; }
     const bool in = xt >= 2 && xt <= p.nx - 3 && yt >= 2 && yt <= p.ny - 3 && zt >= 2 && zt <= p.nz - 3;
-    F[in ? idx + p.push[q] + wrap : opp(q) * N + idx] = Pop<T>::put(f[q]);
+    F[in ? q * N + idx + link_offset(q, sy, sz) + wrap : opp(q) * N + idx] = Pop<T>::put(f[q]);
   }
 }
 
