@@ -75,14 +75,18 @@ __global__ void __launch_bounds__(64) lbib_spread_gather(const double* __restric
 /* Nodes [i0, i1) of the concatenated sheets.  With `box` (an overlapped
  * step's next box), the box in tiles of the moved nodes' stencils is
  * reduced into it (block reduction, then six atomics per block). */
-__global__ void __launch_bounds__(128) lbib_move_nodes(double* __restrict__ nodes, const double* __restrict__ W,
-                                                       const int* __restrict__ st, long i0, long i1, int ntx, int nty,
-                                                       const int* __restrict__ slot, const double* __restrict__ Utile,
-                                                       double dt, const int* err, int* __restrict__ box, int nx,
-                                                       int ny, int nz) {
+constexpr int kMoveTPB = 64;   /* two warps, each with its staged union box */
+
+__global__ void __launch_bounds__(kMoveTPB) lbib_move_nodes(double* __restrict__ nodes, const double* __restrict__ W,
+                                                            const int* __restrict__ st, long i0, long i1, int ntx,
+                                                            int nty, const int* __restrict__ slot,
+                                                            const double* __restrict__ Utile, double dt,
+                                                            const int* err, int* __restrict__ box, int nx, int ny,
+                                                            int nz) {
+  __shared__ double sU[kMoveTPB / 32][3 * kMoveCap + kMoveTiles / 2];   /* + the staged tile slots */
   const long i = i0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < i1 && !*(volatile const int*)err;
-  if (live) move_node(nodes, W, st, i, ntx, nty, slot, Utile, dt);
+  move_warp(nodes, W, st, i, live, ntx, nty, slot, Utile, dt, sU[threadIdx.x >> 5]);
   if (!box) return;
   int b[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN};
   if (live) {
@@ -236,17 +240,18 @@ extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
 extern "C" int lbdev_launch_move(lbib_device* d) {
   const int c = d->cur;
   if (!(d->compat & LBIB_OPT_PIN_ROW0)) {
-    const unsigned nb = (unsigned)((d->S + 127) / 128);
-    lbib_move_nodes<<<nb, 128, 0, d->stream>>>(d->nodes, d->W, d->st, 0, d->S, d->ntx, d->nty, d->tile_slot[c],
-                                               d->Utile[c], (double)d->dt, d->err, d->box_next, d->nx, d->ny,
-                                               d->nz);
+    const unsigned nb = (unsigned)((d->S + kMoveTPB - 1) / kMoveTPB);
+    lbib_move_nodes<<<nb, kMoveTPB, 0, d->stream>>>(d->nodes, d->W, d->st, 0, d->S, d->ntx, d->nty,
+                                                    d->tile_slot[c], d->Utile[c], (double)d->dt, d->err,
+                                                    d->box_next, d->nx, d->ny, d->nz);
     d->kernel_launches++;
   } else {
     for (int k = 0; k < d->nsheets; ++k) {
       const long i0 = d->sh[k].offset + d->sh[k].cols, i1 = d->sh[k].offset + (long)d->sh[k].rows * d->sh[k].cols;
-      const unsigned nb = (unsigned)((i1 - i0 + 127) / 128);
-      lbib_move_nodes<<<nb, 128, 0, d->stream>>>(d->nodes, d->W, d->st, i0, i1, d->ntx, d->nty, d->tile_slot[c],
-                                                 d->Utile[c], (double)d->dt, d->err, nullptr, d->nx, d->ny, d->nz);
+      const unsigned nb = (unsigned)((i1 - i0 + kMoveTPB - 1) / kMoveTPB);
+      lbib_move_nodes<<<nb, kMoveTPB, 0, d->stream>>>(d->nodes, d->W, d->st, i0, i1, d->ntx, d->nty,
+                                                      d->tile_slot[c], d->Utile[c], (double)d->dt, d->err, nullptr,
+                                                      d->nx, d->ny, d->nz);
       d->kernel_launches++;
     }
   }

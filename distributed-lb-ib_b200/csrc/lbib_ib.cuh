@@ -721,6 +721,106 @@ __device__ __forceinline__ void move_node(double* __restrict__ nodes, const doub
 }
 
 
+/* Cells a warp's staged move holds in shared memory: the union box of its
+ * 32 nodes' stencils (along a fiber row ~5 x 20 x 5 cells); a larger
+ * union (a warp straddling two rows, a crumpled sheet) takes move_node. */
+constexpr int kMoveCap = 640;
+constexpr int kMoveTiles = 64;   /* tiles of the union box whose slots are staged */
+
+__device__ __forceinline__ int warp_min(int v) {
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_max(int v) {
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+/* move_node for the 32 nodes of a warp (node i on this lane, `live` if it
+ * moves), with the velocity of the union box of their stencils staged once
+ * in shared memory (sU: 3 x kMoveCap doubles for this warp): the lanes
+ * read each box cell's u from its moment tile with coalesced loads, then
+ * every lane sums its own 64 terms from shared memory -- the same values
+ * in the same order as move_node, with ~5x fewer L2 requests (neighbouring
+ * nodes' stencils overlap by 3 cells of 4).  Called by all 32 lanes. */
+__device__ __forceinline__ void move_warp(double* __restrict__ nodes, const double* __restrict__ W,
+                                          const int* __restrict__ st, long i, bool live, int ntx, int nty,
+                                          const int* __restrict__ slot, const double* __restrict__ Utile, double dt,
+                                          double* __restrict__ sU) {
+  const int lane = threadIdx.x & 31;
+  int is = 0, js = 0, ks = 0;
+  if (live) { is = st[i * 3 + 0]; js = st[i * 3 + 1]; ks = st[i * 3 + 2]; }
+  const int x0 = warp_min(live ? is : INT_MAX), x1 = warp_max(live ? is + 3 : INT_MIN);
+  if (x0 > x1) return;   /* no live lane */
+  const int y0 = warp_min(live ? js : INT_MAX), y1 = warp_max(live ? js + 3 : INT_MIN);
+  const int z0 = warp_min(live ? ks : INT_MAX), z1 = warp_max(live ? ks + 3 : INT_MIN);
+  const int bx = x1 - x0 + 1, by = y1 - y0 + 1, bz = z1 - z0 + 1;
+  const long vol = (long)bx * by * bz;
+  const int ntiles_box = ((x1 >> 2) - (x0 >> 2) + 1) * ((y1 >> 2) - (y0 >> 2) + 1) * ((z1 >> 2) - (z0 >> 2) + 1);
+  if (vol > kMoveCap || ntiles_box > kMoveTiles) {   /* uniform over the warp */
+    if (live) move_node(nodes, W, st, i, ntx, nty, slot, Utile, dt);
+    return;
+  }
+  /* the slots of the box's tiles first (at most 3 x 7 x 3 for a box that
+     fits), so that the cell loads below depend on one shared-memory read */
+  int* sslot = reinterpret_cast<int*>(sU + 3 * kMoveCap);
+  const int tx0 = x0 >> 2, ty0 = y0 >> 2, tz0 = z0 >> 2;
+  const int tbx = (x1 >> 2) - tx0 + 1, tby = (y1 >> 2) - ty0 + 1, ntb = tbx * tby * ((z1 >> 2) - tz0 + 1);
+  for (int j = lane; j < ntb; j += 32) {
+    const int tx = tx0 + j % tbx, ty = ty0 + (j / tbx) % tby, tz = tz0 + j / (tbx * tby);
+    sslot[j] = slot[(tz * nty + ty) * ntx + tx];
+  }
+  __syncwarp();
+  /* the box's longest axis (the fiber direction: neighbouring lanes'
+     stencils are offset along it) is stored fastest, so that the lanes'
+     reads below fall on consecutive words, not on one bank */
+  const int f = (bx >= by && bx >= bz) ? 0 : (by >= bz ? 1 : 2);
+  const int a = f == 0 ? 1 : 0, b = f == 2 ? 1 : 2;
+  const int ext[3] = {bx, by, bz};
+  int str[3];
+  str[f] = 1; str[a] = ext[f]; str[b] = ext[f] * ext[a];
+#pragma unroll 4
+  for (int j = lane; j < (int)vol; j += 32) {
+    int u[3];
+    u[f] = j % ext[f]; u[a] = (j / ext[f]) % ext[a]; u[b] = j / (ext[f] * ext[a]);
+    const int cx = x0 + u[0], cy = y0 + u[1], cz = z0 + u[2];
+    /* a box corner no stencil covers may lie in an untouched tile: never read */
+    const int sp = sslot[((cz >> 2) - tz0) * tbx * tby + ((cy >> 2) - ty0) * tbx + ((cx >> 2) - tx0)];
+    double vx = 0.0, vy = 0.0, vz = 0.0;
+    if (sp >= 0) {
+      const double* U = Utile + (long)sp * 256;
+      const int cell = lbib::cell_in_tile(cx, cy, cz);
+      vx = U[64 + cell]; vy = U[128 + cell]; vz = U[192 + cell];
+    }
+    sU[j] = vx; sU[kMoveCap + j] = vy; sU[2 * kMoveCap + j] = vz;
+  }
+  __syncwarp();
+  if (live) {
+    const double c_64 = 1.0 / (6.4e1);
+    const double* w = W + i * 12;
+    double s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+    for (int i2 = 0; i2 <= 3; i2++) {
+#pragma unroll
+      for (int j2 = 0; j2 <= 3; j2++) {
+#pragma unroll
+        for (int k2 = 0; k2 <= 3; k2++) {
+          const int c = (is + i2 - x0) * str[0] + (js + j2 - y0) * str[1] + (ks + k2 - z0) * str[2];
+          const double vx = sU[c], vy = sU[kMoveCap + c], vz = sU[2 * kMoveCap + c];
+          s1 += vx * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
+          s2 += vy * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
+          s3 += vz * w[i2] * w[4 + j2] * w[8 + k2] * c_64;
+        }
+      }
+    }
+    double* m = nodes + i * 12;
+    m[0] += dt * s1;
+    m[1] += dt * s2;
+    m[2] += dt * s3;
+  }
+  __syncwarp();
+}
+
 }  // namespace lbib
 
 #endif
