@@ -22,6 +22,7 @@ int lbdev_launch_init(lbib_device* d, int what);
 int lbdev_launch_sums(lbib_device* d, double* part, double* out);
 int lbdev_lp_variants(int prec);
 int lbdev_launch_fiber_forces(lbib_device* d, int k);
+int lbdev_can_fuse_forces(const lbib_device* d);
 int lbdev_launch_spread(lbib_device* d, int step);
 int lbdev_launch_move(lbib_device* d);
 int lbdev_launch_stencil_box(lbib_device* d);
@@ -462,9 +463,12 @@ static int step_overlapped(lbib_device* d, int step_no, cudaEvent_t* ev) {
   cudaStream_t fs = conc ? d->side : d->stream;
   int rc = 0;
   if (!conc) {
-    for (int k = 0; k < d->nsheets && !rc; ++k) rc = lbdev_launch_fiber_forces(d, k);
+    /* the forces: in the node preparation's launch when the sheets allow */
+    d->fuse_forces = lbdev_can_fuse_forces(d);
+    for (int k = 0; k < d->nsheets && !rc && !d->fuse_forces; ++k) rc = lbdev_launch_fiber_forces(d, k);
     if (ev) CK(cudaEventRecord(ev[1], d->stream));
     if (!rc) rc = lbdev_launch_spread(d, step_no);
+    d->fuse_forces = 0;
     if (ev) CK(cudaEventRecord(ev[2], d->stream));
     if (rc) { d->box_mode = 0; d->box_next = NULL; d->box_valid = 0; return -2; }
   }

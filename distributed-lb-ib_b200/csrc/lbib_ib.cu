@@ -18,14 +18,35 @@ __global__ void lbib_fiber_forces(double* __restrict__ nodes, int R, int C, doub
   fiber_forces_node(nodes, R, C, bc, sc, sc2, ds1, ds2, bend_bug, i);
 }
 
-/* A block per 32-node chunk: warp p evaluates part p of the chunk's nodes
- * (node_prep_part); warp 0 also reduces the chunk's stencil box. */
-__global__ void __launch_bounds__(128) lbib_node_prep(const double* __restrict__ nodes, long S, int nx, int ny, int nz,
+/* The sheets whose fiber forces the node preparation computes as well
+ * (n = 0: none; the forces then come from lbib_fiber_forces). */
+constexpr int kFuseSheets = 4;
+struct SheetForces {
+  int n, bend_bug;
+  lbib_sheet_dev s[kFuseSheets];
+};
+
+/* A block per 32-node chunk: warp p < 4 evaluates part p of the chunk's
+ * nodes (node_prep_part); warp 0 also reduces the chunk's stencil box.  A
+ * fifth warp, when the block has one, computes the nodes' fiber forces for
+ * the sheets `sf` names (fiber_forces_node reads neighbours' positions and
+ * writes the node's own force fields only, so it runs alongside). */
+__global__ void __launch_bounds__(160) lbib_node_prep(double* __restrict__ nodes, long S, int nx, int ny, int nz,
                                                       int ntx, int nty, double* __restrict__ W, int* __restrict__ st,
                                                       int* __restrict__ tile_cnt, int* __restrict__ chunk_box, int* err,
-                                                      int step) {
+                                                      int step, SheetForces sf) {
   const long i = (long)blockIdx.x * 32 + (threadIdx.x & 31);
   const int part = threadIdx.x >> 5;
+  if (part == 4) {
+    if (sf.n == 0 || i >= S) return;
+    int k = 0;
+    while (k + 1 < sf.n && i >= sf.s[k + 1].offset) ++k;
+    const lbib_sheet_dev& h = sf.s[k];
+    const long li = i - h.offset;
+    if (li < (long)h.rows * h.cols)
+      fiber_forces_node(nodes + h.offset * 12, h.rows, h.cols, h.bc, h.sc, h.sc2, h.ds1, h.ds2, sf.bend_bug, (int)li);
+    return;
+  }
   int b0 = INT_MAX, b1 = INT_MIN, b2 = INT_MAX, b3 = INT_MIN, b4 = INT_MAX, b5 = INT_MIN;
   if (i < S) node_prep_part(nodes, i, part, nx, ny, nz, ntx, nty, W, st, tile_cnt, err, step, b0, b1, b2, b3, b4, b5);
   if (part == 0) chunk_box_reduce(i, S, chunk_box, b0, b1, b2, b3, b4, b5);
@@ -206,6 +227,10 @@ extern "C" int lbdev_launch_stencil_box(lbib_device* d) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+/* The fiber forces fold into the node preparation for up to kFuseSheets
+ * sheets: lbdev_launch_spread computes them when d->fuse_forces is set. */
+extern "C" int lbdev_can_fuse_forces(const lbib_device* d) { return d->nsheets <= kFuseSheets; }
+
 extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
   const int c = d->cur;
   cudaStream_t st = d->stream;
@@ -213,8 +238,16 @@ extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
      compaction, so the step needs no clearing pass */
   const long S = d->S;
   const unsigned nb = (unsigned)((S + 127) / 128);
-  lbib_node_prep<<<(unsigned)d->nchunks, 128, 0, st>>>(d->nodes, S, d->nx, d->ny, d->nz, d->ntx, d->nty, d->W, d->st,
-                                                       d->tile_cnt, d->chunk_box, d->err, step);
+  SheetForces sf;
+  sf.n = 0;
+  sf.bend_bug = (d->compat & 1) != 0;
+  if (d->fuse_forces && d->nsheets <= kFuseSheets) {
+    sf.n = d->nsheets;
+    for (int k = 0; k < d->nsheets; ++k) sf.s[k] = d->sh[k];
+  }
+  lbib_node_prep<<<(unsigned)d->nchunks, sf.n ? 160 : 128, 0, st>>>(d->nodes, S, d->nx, d->ny, d->nz, d->ntx, d->nty,
+                                                                    d->W, d->st, d->tile_cnt, d->chunk_box, d->err,
+                                                                    step, sf);
   const unsigned nblk = (unsigned)((d->ntiles + kScanBlock - 1) / kScanBlock);
   int* block_tiles = d->scan_tmp;
   int* block_pairs = d->scan_tmp + nblk + 1;

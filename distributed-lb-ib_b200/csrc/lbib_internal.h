@@ -146,6 +146,7 @@ typedef struct lbib_device {
   int* box_next;                 /* the move accumulates the next box here    */
   int box_mode;                  /* 1 inside an overlapped step               */
   int overlap;                   /* overlapped steps allowed (LBIB_OVERLAP)   */
+  int fuse_forces;               /* the spread's node preparation also computes the fiber forces */
   int device;
   long kernel_launches;          /* kernels this state has launched           */
   /* optional stage timing: events around the five stages of each step */
