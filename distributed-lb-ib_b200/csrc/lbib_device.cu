@@ -49,6 +49,7 @@ static void free_tiles(lbib_device* d) {
   cudaFree(d->slot_cursor); d->slot_cursor = NULL;
   cudaFree(d->pair_node); d->pair_node = NULL;
   cudaFree(d->scan_tmp); d->scan_tmp = NULL;
+  cudaFree(d->scan_state); d->scan_state = NULL;
 }
 
 static void free_sheets(lbib_device* d) {
@@ -339,6 +340,8 @@ extern "C" int lbdev_set_sheets(lbib_device* d, int nsheets, const lbib_sheet_de
     CK(cudaMalloc(&d->slot_cursor, sizeof(int) * d->cap));
     CK(cudaMalloc(&d->pair_node, sizeof(int2) * 8 * S));
     CK(cudaMalloc(&d->scan_tmp, sizeof(int) * 2 * ((d->ntiles + 1023) / 1024 + 1)));
+    CK(cudaMalloc(&d->scan_state, sizeof(unsigned long long) * ((d->ntiles + 1023) / 1024 + 1)));
+    CK(cudaMemsetAsync(d->scan_state, 0, sizeof(unsigned long long) * ((d->ntiles + 1023) / 1024 + 1), d->stream));
   }
   free(d->sh);
   d->sh = (lbib_sheet_dev*)malloc(sizeof(lbib_sheet_dev) * nsheets);

@@ -249,12 +249,21 @@ extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
                                                                     d->W, d->st, d->tile_cnt, d->chunk_box, d->err,
                                                                     step, sf);
   const unsigned nblk = (unsigned)((d->ntiles + kScanBlock - 1) / kScanBlock);
-  int* block_tiles = d->scan_tmp;
-  int* block_pairs = d->scan_tmp + nblk + 1;
-  lbib_compact_count<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, block_tiles, block_pairs);
-  lbib_compact_scan<<<1, kScanBlock, 0, st>>>(block_tiles, block_pairs, (int)nblk, d->tile_count[c]);
-  lbib_compact_write<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, block_tiles, block_pairs, d->tile_list[c],
-                                                  d->tile_slot[c], d->slot_off, d->slot_len, d->slot_cursor);
+  if (d->scan_state && d->ntiles < (1L << 22) && 8 * S < (1L << 31)) {
+    d->scan_tag = d->scan_tag % 255u + 1u;
+    lbib_compact_onepass<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, (int)nblk, d->scan_state, d->scan_tag,
+                                                      d->tile_list[c], d->tile_slot[c], d->slot_off, d->slot_len,
+                                                      d->slot_cursor, d->tile_count[c], d->err);
+    d->kernel_launches -= 2;
+  } else {
+    int* block_tiles = d->scan_tmp;
+    int* block_pairs = d->scan_tmp + nblk + 1;
+    lbib_compact_count<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, block_tiles, block_pairs);
+    lbib_compact_scan<<<1, kScanBlock, 0, st>>>(block_tiles, block_pairs, (int)nblk, d->tile_count[c]);
+    lbib_compact_write<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, block_tiles, block_pairs,
+                                                    d->tile_list[c], d->tile_slot[c], d->slot_off, d->slot_len,
+                                                    d->slot_cursor);
+  }
   /* an x-slab lists and gathers the tiles of its own columns only */
   const int tlo = d->x_lo / 4, thi = (d->x_hi + 3) / 4;
   int2* ent = reinterpret_cast<int2*>(d->pair_node);

@@ -335,6 +335,126 @@ static __global__ void lbib_compact_write(int* __restrict__ cnt, long n, const i
   if (i < n && c) cnt[i] = 0;   /* counts start the next step at zero */
 }
 
+/* The same compaction in one launch: a single-pass scan with decoupled
+ * look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan with
+ * Decoupled Look-back", 2016).  A block takes its place in tile order from
+ * a ticket counter (so every block before it has started), publishes its
+ * block totals, walks back over its predecessors' published totals until
+ * one carries an inclusive prefix, publishes its own inclusive prefix and
+ * writes its tiles' slots.  Each published word is 64 bits: an 8-bit
+ * launch tag (1..255, never 0, so a zeroed or stale word never matches),
+ * a 2-bit flag (1 block totals, 2 inclusive prefix), 22 bits of tiles and
+ * 32 bits of pairs; the host uses it only when the tile count fits 22
+ * bits.  Every wait is bounded: a walk that runs out sets err (the step
+ * then fails) instead of spinning on.  state[nblk] holds the ticket,
+ * which the last block resets for the next launch. */
+constexpr long kLookbackSpin = 1L << 22;
+constexpr int kErrLookback = -2;   /* the error word's code: LBIB_E_CUDA of include/lbib.h */
+
+__device__ __forceinline__ unsigned long long lookback_word(unsigned tag, unsigned flag, unsigned long long t,
+                                                            unsigned long long p) {
+  return ((unsigned long long)tag << 56) | ((unsigned long long)flag << 54) | ((t & 0x3FFFFFull) << 32) |
+         (p & 0xFFFFFFFFull);
+}
+
+static __global__ void __launch_bounds__(kScanBlock) lbib_compact_onepass(int* __restrict__ cnt, long n, int nblk,
+                                                                          unsigned long long* __restrict__ state,
+                                                                          unsigned tag, int* __restrict__ list,
+                                                                          int* __restrict__ slot,
+                                                                          int* __restrict__ slot_off,
+                                                                          int* __restrict__ slot_len,
+                                                                          int* __restrict__ slot_cursor,
+                                                                          int* __restrict__ total, int* err) {
+  __shared__ int sv[32], sw[32];
+  __shared__ int s_vb, s_tt, s_tp, s_pt, s_pp;
+  unsigned* ticket = reinterpret_cast<unsigned*>(state + nblk);
+  if (threadIdx.x == 0) s_vb = (int)atomicAdd(ticket, 1u);
+  __syncthreads();
+  const int vb = s_vb;
+  const long i = (long)vb * kScanBlock + threadIdx.x;
+  const int c = (i < n) ? cnt[i] : 0;
+  const int v = c > 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int iv = v, iw = c;  /* inclusive warp scans */
+  for (int o = 1; o < 32; o <<= 1) {
+    const int tv = __shfl_up_sync(0xffffffffu, iv, o);
+    const int tw = __shfl_up_sync(0xffffffffu, iw, o);
+    if (lane >= o) { iv += tv; iw += tw; }
+  }
+  if (lane == 31) { sv[warp] = iv; sw[warp] = iw; }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int a = sv[threadIdx.x], b = sw[threadIdx.x];
+    int ia = a, ib = b;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ta = __shfl_up_sync(0xffffffffu, ia, o);
+      const int tb = __shfl_up_sync(0xffffffffu, ib, o);
+      if (lane >= o) { ia += ta; ib += tb; }
+    }
+    sv[threadIdx.x] = ia - a;
+    sw[threadIdx.x] = ib - b;
+    if (threadIdx.x == 31) { s_tt = ia; s_tp = ib; }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    /* warp 0 walks back 32 predecessors at a time: lane k reads block
+       j - k; the window is summed up to its nearest inclusive word once
+       every word up to there has been published */
+    volatile unsigned long long* vs = state;
+    const unsigned long long at = (unsigned)s_tt, ap = (unsigned)s_tp;
+    if (vb > 0 && lane == 0) vs[vb] = lookback_word(tag, 1u, at, ap);
+    __syncwarp();
+    unsigned long long et = 0, ep = 0;
+    long spins = 0;
+    for (int j = vb - 1; j >= 0;) {
+      const int jj = j - lane;
+      const unsigned long long w = jj >= 0 ? vs[jj] : lookback_word(tag, 2u, 0ull, 0ull);
+      const unsigned f = (unsigned)(w >> 54) & 3u;
+      const bool ready = (unsigned)(w >> 56) == tag && f != 0u;
+      const unsigned incl = __ballot_sync(0xffffffffu, ready && f == 2u);
+      const unsigned rdy = __ballot_sync(0xffffffffu, ready);
+      const int lim = incl ? __ffs(incl) - 1 : 31;
+      const unsigned need = lim == 31 ? 0xffffffffu : (1u << (lim + 1)) - 1u;
+      if ((rdy & need) != need) {
+        if (++spins > kLookbackSpin) {
+          if (lane == 0) atomicCAS(err, 0, kErrLookback);
+          break;
+        }
+        continue;
+      }
+      unsigned long long t = lane <= lim ? (w >> 32) & 0x3FFFFFull : 0ull;
+      unsigned long long q = lane <= lim ? w & 0xFFFFFFFFull : 0ull;
+      for (int o = 16; o > 0; o >>= 1) {
+        t += __shfl_xor_sync(0xffffffffu, t, o);
+        q += __shfl_xor_sync(0xffffffffu, q, o);
+      }
+      et += t; ep += q;
+      if (incl) break;
+      j -= 32;
+    }
+    if (lane == 0) {
+      vs[vb] = lookback_word(tag, 2u, et + at, ep + ap);
+      s_pt = (int)et; s_pp = (int)ep;
+      if (vb == nblk - 1) {
+        *total = (int)(et + at);
+        *ticket = 0u;   /* every block has taken its ticket */
+      }
+    }
+  }
+  __syncthreads();
+  if (v) {
+    const int pos = s_pt + sv[warp] + iv - v;
+    list[pos] = (int)i;
+    slot[i] = pos;
+    slot_off[pos] = s_pp + sw[warp] + iw - c;
+    slot_len[pos] = c;
+    slot_cursor[pos] = 0;
+  } else if (i < n) {
+    slot[i] = -1;     /* the whole map is written: no clearing pass before the step */
+  }
+  if (i < n && c) cnt[i] = 0;   /* counts start the next step at zero */
+}
+
 /* Every node appends its index to the list of each tile its stencil touches
  * (order within a list is fixed afterwards by sorting). */
 __device__ __forceinline__ void pair_scatter_one(const int* __restrict__ st, long i, int ntx, int nty, int nx, int ny,

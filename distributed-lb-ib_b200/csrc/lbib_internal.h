@@ -110,6 +110,8 @@ typedef struct lbib_device {
   int* tile_list[2];             /* [cap] touched tiles in index order        */
   int* tile_count[2];            /* [1]                                       */
   int* scan_tmp;                 /* block sums for the compaction             */
+  unsigned long long* scan_state; /* one-pass compaction: per-block words + ticket */
+  unsigned scan_tag;             /* the one-pass compaction's launch tag (1..255) */
   double* Ftile[2];              /* [cap][3][64]                              */
   double* Utile[2];              /* [cap][4][64]                              */
   int cur;                       /* buffers of the step in progress / last    */
