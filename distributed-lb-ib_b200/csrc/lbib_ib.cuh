@@ -711,10 +711,20 @@ __device__ __forceinline__ void gather_tile_ent(GatherSmemE& sm, const double* _
       sm.m32[1][t] = (unsigned)(m >> 32);
     }
     __syncthreads();
-    for (int j = 0; j < nb; ++j) {
-      const unsigned m = mw[j];
-      if (m == 0u) continue;
-      if ((m >> lane) & 1u) {
+    /* 32 nodes at a time: the warp's 32 x 32 cover bits (node j covers
+       lane l's cell) are transposed with five shuffle stages, so that
+       each lane walks only the nodes that cover its cell, in node order */
+    for (int j0 = 0; j0 < nb; j0 += 32) {
+      unsigned x = j0 + lane < nb ? mw[j0 + lane] : 0u;
+#pragma unroll
+      for (int k = 16; k >= 1; k >>= 1) {
+        const unsigned M = k == 16 ? 0x0000FFFFu : k == 8 ? 0x00FF00FFu : k == 4 ? 0x0F0F0F0Fu
+                         : k == 2 ? 0x33333333u : 0x55555555u;
+        const unsigned y = __shfl_xor_sync(0xffffffffu, x, k);
+        x = (lane & k) ? (x & ~M) | ((y & ~M) >> k) : (x & M) | ((y & M) << k);
+      }
+      for (unsigned bits = x; bits; bits &= bits - 1u) {
+        const int j = j0 + __ffs(bits) - 1;
         const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
         const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
         Fx = Fx + s_fe[j][0] * tmp;
