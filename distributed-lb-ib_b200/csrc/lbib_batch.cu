@@ -72,68 +72,72 @@ __global__ void lbib_b_node_prep(const double* __restrict__ nodes, const int* __
   chunk_box_reduce(i, SP, chunk_box, b0, b1, b2, b3, b4, b5);
 }
 
+/* Entries {chunk, lane mask} per tile, as the one-grid spread's: a warp's
+ * 32 nodes belong to one problem (every problem's nodes start at a
+ * multiple of 32), so the warp works with that problem's grid; warps of
+ * padding nodes or of a failed problem append nothing. */
 __global__ void lbib_b_pair_scatter(const int* __restrict__ st, const int* __restrict__ node_inst,
                                     const BatchDesc* __restrict__ D, const int* __restrict__ slot,
                                     const int* __restrict__ slot_off, int* __restrict__ slot_cursor,
-                                    int* __restrict__ pair_node, const int* err, long SP) {
+                                    int2* __restrict__ ent, const int* err, long SP) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= SP) return;
-  const int k = node_inst[i];
-  if (k < 0 || *(volatile const int*)(err + 2 * k)) return;
+  const long i0 = i & ~31L;   /* the warp's first node: its problem is the warp's */
+  const int k = i0 < SP ? node_inst[i0] : -1;
+  if (k < 0 || *(volatile const int*)(err + 2 * k)) return;   /* uniform over the warp */
   const BatchDesc& d = D[k];
-  pair_scatter_one(st, i, d.ntx, d.nty, d.nx, d.ny, d.nz, slot + d.tile0, slot_off, slot_cursor, pair_node);
+  const long S = i < SP && node_inst[i] == k ? i + 1 : i;   /* lanes past the problem's nodes: no node */
+  pair_scatter_warp(st, i, S, d.ntx, d.nty, d.nx, d.ny, d.nz, 0, d.ntx, slot + d.tile0, slot_off, slot_cursor, ent);
 }
 
+/* Every listed tile of the batch from its entries (gather_tile_ent), or,
+ * with more than kListCap nodes, by scanning its problem's node chunks in
+ * order (gather_tile_scan), in one launch. */
 __global__ void __launch_bounds__(64) lbib_b_gather(const double* __restrict__ nodes, const double* __restrict__ W,
-                                                    const int* __restrict__ st, const int* __restrict__ list,
-                                                    const int* __restrict__ count, const int* __restrict__ slot_off,
-                                                    const int* __restrict__ slot_len, const int* __restrict__ pair_node,
+                                                    const int* __restrict__ st, const int* __restrict__ chunk_box,
+                                                    const int* __restrict__ list, const int* __restrict__ count,
+                                                    const int* __restrict__ slot_off, const int* __restrict__ slot_len,
+                                                    const int* __restrict__ slot_cursor, const int2* __restrict__ ent,
                                                     const int* __restrict__ tile_inst, const BatchDesc* __restrict__ D,
                                                     double* __restrict__ Ftile, const int* err) {
-  __shared__ GatherSmem sm;
+  __shared__ union {
+    GatherSmemE e;
+    ScanSmem s;
+  } sm;
   const int n = *count;
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
     const int tile = list[it];
     const int k = tile_inst[tile];
     if (*(volatile const int*)(err + 2 * k)) continue;
     const BatchDesc& d = D[k];
-    gather_tile(sm, nodes, W, st, it, (int)(tile - d.tile0), slot_off, slot_len, pair_node, d.ntx, d.nty, Ftile);
+    const int L = slot_len[it];
+    if (L <= kListCap) {
+      gather_tile_ent(sm.e, nodes, W, st, it, (int)(tile - d.tile0), L, slot_cursor[it], ent + slot_off[it], d.ntx,
+                      d.nty, Ftile);
+    } else {
+      __syncthreads();   /* the union's previous contents are no longer read */
+      const long end = d.node0 + d.S;
+      gather_tile_scan(sm.s, nodes, W, st, chunk_box, end, d.node0 >> 5, (end + 31) >> 5, it, (int)(tile - d.tile0),
+                       d.ntx, d.nty, Ftile);
+    }
   }
 }
 
-__global__ void __launch_bounds__(64) lbib_b_gather_scan(const double* __restrict__ nodes, const double* __restrict__ W,
-                                                         const int* __restrict__ st, const int* __restrict__ chunk_box,
-                                                         const int* __restrict__ list, const int* __restrict__ count,
-                                                         const int* __restrict__ slot_len,
-                                                         const int* __restrict__ tile_inst,
-                                                         const BatchDesc* __restrict__ D, double* __restrict__ Ftile,
-                                                         const int* err) {
-  __shared__ ScanSmem sm;
-  const int n = *count;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    if (slot_len[it] <= kListCap) continue;
-    const int tile = list[it];
-    const int k = tile_inst[tile];
-    if (*(volatile const int*)(err + 2 * k)) continue;
-    const BatchDesc& d = D[k];
-    const long end = d.node0 + d.S;
-    gather_tile_scan(sm, nodes, W, st, chunk_box, end, d.node0 >> 5, (end + 31) >> 5, it, (int)(tile - d.tile0),
-                     d.ntx, d.nty, Ftile);
-  }
-}
-
-__global__ void lbib_b_move(double* __restrict__ nodes, const double* __restrict__ W, const int* __restrict__ st,
-                            const int* __restrict__ node_inst, const BatchDesc* __restrict__ D,
-                            const int* __restrict__ slot, const double* __restrict__ Utile, const int* err, long SP,
-                            int* __restrict__ step_no) {
+/* The move, a warp per 32 nodes of one problem with the union box of their
+ * stencils staged in shared memory (move_warp); a pinned leading row stays. */
+__global__ void __launch_bounds__(64) lbib_b_move(double* __restrict__ nodes, const double* __restrict__ W,
+                                                  const int* __restrict__ st, const int* __restrict__ node_inst,
+                                                  const BatchDesc* __restrict__ D, const int* __restrict__ slot,
+                                                  const double* __restrict__ Utile, const int* err, long SP,
+                                                  int* __restrict__ step_no) {
+  __shared__ double sU[2][3 * kMoveCap + kMoveTiles / 2];
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) ++*step_no;   /* the last kernel of the step; node_prep has read it */
-  if (i >= SP) return;
-  const int k = node_inst[i];
-  if (k < 0 || *(volatile const int*)(err + 2 * k)) return;
+  const long i0 = i & ~31L;
+  const int k = i0 < SP ? node_inst[i0] : -1;
+  if (k < 0 || *(volatile const int*)(err + 2 * k)) return;   /* uniform over the warp */
   const BatchDesc& d = D[k];
-  if (d.pinned && i - d.node0 < d.cols) return;
-  move_node(nodes, W, st, i, d.ntx, d.nty, slot + d.tile0, Utile, d.dt);
+  const bool live = i < SP && node_inst[i] == k && !(d.pinned && i - d.node0 < d.cols);
+  move_warp(nodes, W, st, i, live, d.ntx, d.nty, slot + d.tile0, Utile, d.dt, sU[threadIdx.x >> 5]);
 }
 
 /* FP64 rows away from the walls: the two-cell step, a block per 128 pairs of
@@ -408,14 +412,13 @@ int batch_step(lbib_batch* b) {
   lbib_compact_scan<<<1, kScan, 0, s>>>(block_tiles, block_pairs, (int)nblk, b->tile_count[c]);
   lbib_compact_write<<<nblk, kScan, 0, s>>>(b->tile_cnt, b->NT, block_tiles, block_pairs, b->tile_list[c],
                                             b->tile_slot[c], b->slot_off, b->slot_len, b->slot_cursor);
+  int2* ent = reinterpret_cast<int2*>(b->pair_node);
   lbib_b_pair_scatter<<<nb, 128, 0, s>>>(b->st, b->node_inst, b->desc, b->tile_slot[c], b->slot_off, b->slot_cursor,
-                                         b->pair_node, b->err, SP);
-  lbib_b_gather<<<b->grid_tiles, 64, 0, s>>>(b->nodes, b->W, b->st, b->tile_list[c], b->tile_count[c], b->slot_off,
-                                             b->slot_len, b->pair_node, b->tile_inst, b->desc, b->Ftile[c], b->err);
-  lbib_b_gather_scan<<<b->grid_tiles / 4 + 1, 64, 0, s>>>(b->nodes, b->W, b->st, b->chunk_box, b->tile_list[c],
-                                                          b->tile_count[c], b->slot_len, b->tile_inst, b->desc,
-                                                          b->Ftile[c], b->err);
-  b->launches += 9;
+                                         ent, b->err, SP);
+  lbib_b_gather<<<b->grid_tiles, 64, 0, s>>>(b->nodes, b->W, b->st, b->chunk_box, b->tile_list[c], b->tile_count[c],
+                                             b->slot_off, b->slot_len, b->slot_cursor, ent, b->tile_inst, b->desc,
+                                             b->Ftile[c], b->err);
+  b->launches += 8;
   /* the fused fluid step */
   const void* P = first ? b->P_first : b->P[c];
   const void* WP = first ? b->WP_first : b->WP[c];
@@ -435,8 +438,8 @@ int batch_step(lbib_batch* b) {
   /* moments of the touched tiles, read by the next step and the move */
   BatchFluid g = fluid_args(b, par ^ 1, b->P[c], b->WP[c], c);
   if ((is_lp(b) ? batch_tile_moments_lp(g) : batch_tile_moments_f64(g))) return -2;
-  lbib_b_move<<<nb, 128, 0, s>>>(b->nodes, b->W, b->st, b->node_inst, b->desc, b->tile_slot[c], b->Utile[c], b->err,
-                                 SP, b->step_no);
+  lbib_b_move<<<(unsigned)((SP + 63) / 64), 64, 0, s>>>(b->nodes, b->W, b->st, b->node_inst, b->desc, b->tile_slot[c],
+                                                        b->Utile[c], b->err, SP, b->step_no);
   b->launches += 2;
   b->cur = c;
   b->parity ^= 1;
@@ -583,7 +586,7 @@ lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision
   if (!rc && cudaMalloc(&b->slot_off, sizeof(int) * CAP) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&b->slot_len, sizeof(int) * CAP) != cudaSuccess) rc = -5;
   if (!rc && cudaMalloc(&b->slot_cursor, sizeof(int) * CAP) != cudaSuccess) rc = -5;
-  if (!rc && cudaMalloc(&b->pair_node, sizeof(int) * 8 * SP) != cudaSuccess) rc = -5;
+  if (!rc && cudaMalloc(&b->pair_node, sizeof(int2) * 8 * SP) != cudaSuccess) rc = -5;
   for (int c = 0; c < 2 && !rc; ++c) {
     if (cudaMalloc(&b->tile_slot[c], sizeof(int) * NT) != cudaSuccess) rc = -5;
     if (!rc && cudaMalloc(&b->tile_list[c], sizeof(int) * CAP) != cudaSuccess) rc = -5;

@@ -12,19 +12,21 @@
  *                       tiles the stencil touches; chunk_box_reduce: per
  *                       32-node chunk the bounding box of its stencils.
  *   compaction kernels  touched tiles -> dense list in tile order, tile ->
- *                       slot map, and each slot's node-list offset
- *                       (deterministic prefix sums); pair_scatter_one fills
- *                       the lists.
- *   gather_tile         fiber_SpreadForce + fluid_get_SpreadForce
+ *                       slot map, and each slot's list offset
+ *                       (deterministic prefix sums, three launches or one
+ *                       single-pass launch); pair_scatter_warp fills the
+ *                       lists with {chunk, lane mask} entries.
+ *   gather_tile_ent     fiber_SpreadForce + fluid_get_SpreadForce
  *                       (lbm_ib.c:1323-1525) as a gather: one CTA per touched
- *                       tile sorts the tile's node list by node index in
- *                       shared memory, then each thread (cell) sums the
+ *                       tile sorts the tile's entries, writes its node list
+ *                       in index order, then each thread (cell) sums the
  *                       contributions in that order -- the reference's
  *                       (sheet, row, col) order -- so the result is
  *                       deterministic and needs no atomics on forces.
- *   move_node           moveFiberSheet (lbm_ib.c:2540-2723): u * w summed over
- *                       the 64 stencil cells in the reference's (x, y, z)
- *                       order, then X += dt U.
+ *   move_node /         moveFiberSheet (lbm_ib.c:2540-2723): u * w summed over
+ *   move_warp           the 64 stencil cells in the reference's (x, y, z)
+ *                       order, then X += dt U (move_warp: a warp's nodes
+ *                       with their stencils' union staged in shared memory).
  * All arithmetic keeps the reference's operation order; translation units
  * that include this file are compiled with -fmad=false.
  */
@@ -455,22 +457,6 @@ static __global__ void __launch_bounds__(kScanBlock) lbib_compact_onepass(int* _
   if (i < n && c) cnt[i] = 0;   /* counts start the next step at zero */
 }
 
-/* Every node appends its index to the list of each tile its stencil touches
- * (order within a list is fixed afterwards by sorting). */
-__device__ __forceinline__ void pair_scatter_one(const int* __restrict__ st, long i, int ntx, int nty, int nx, int ny,
-                                                 int nz, const int* __restrict__ slot, const int* __restrict__ slot_off,
-                                                 int* __restrict__ slot_cursor, int* __restrict__ pair_node) {
-  const int is = st[i * 3 + 0], js = st[i * 3 + 1], ks = st[i * 3 + 2];
-  if (is < 0 || is + 3 >= nx || js < 0 || js + 3 >= ny || ks < 0 || ks + 3 >= nz) return;
-  for (int tz = ks >> 2; tz <= (ks + 3) >> 2; ++tz)
-    for (int ty = js >> 2; ty <= (js + 3) >> 2; ++ty)
-      for (int tx = is >> 2; tx <= (is + 3) >> 2; ++tx) {
-        const int s = slot[((long)tz * nty + ty) * ntx + tx];
-        const int k = atomicAdd(&slot_cursor[s], 1);
-        pair_node[slot_off[s] + k] = (int)i;
-      }
-}
-
 /* The one-grid spread's lists hold entries instead of node indices: the
  * nodes of a warp (32 consecutive nodes, chunk i >> 5) that touch a tile
  * at the same stencil offset append one entry {chunk, lane mask} with one
@@ -509,15 +495,6 @@ __device__ __forceinline__ void pair_scatter_warp(const int* __restrict__ st, lo
  * chunk-scan path below. */
 constexpr int kListCap = 1024;
 
-/* Shared memory of one gather CTA (64 threads = one 4^3 tile). */
-struct GatherSmem {
-  int ids[kListCap];
-  int st[64][3];
-  double w[64][12];
-  double fe[64][3];
-  unsigned m32[2][64];   /* per node: the cells of warp 0 / warp 1 its stencil covers */
-};
-
 /* The columns [d, d + 3] of a stencil that starts d cells from a tile's
  * origin, as a 4-bit mask of the tile's columns 0..3 (0 when |d| > 3). */
 __device__ __forceinline__ unsigned span4(int d) {
@@ -536,80 +513,6 @@ __device__ __forceinline__ unsigned long long stencil_tile_mask(int dx, int dy, 
 #pragma unroll
   for (int k = 0; k < 4; ++k) m |= ((mz >> k) & 1u) ? (unsigned long long)row << (16 * k) : 0ull;
   return m;
-}
-
-/* Slot `it` (local tile `tile` of a grid with ntx x nty tiles per z layer):
- * sort its node list, then each of the 64 threads sums its cell's
- * contributions in node order into Ftile[it]. */
-__device__ __forceinline__ void gather_tile(GatherSmem& sm, const double* __restrict__ nodes,
-                                            const double* __restrict__ W, const int* __restrict__ st, int it, int tile,
-                                            const int* __restrict__ slot_off, const int* __restrict__ slot_len,
-                                            const int* __restrict__ pair_node, int ntx, int nty,
-                                            double* __restrict__ Ftile) {
-  int* ids = sm.ids;
-  auto& s_st = sm.st;
-  auto& s_w = sm.w;
-  auto& s_fe = sm.fe;
-  const int t = threadIdx.x;
-  const double cf = 1.0 / (64.0 * 1.0 * 1.0 * 1.0);
-  {
-    const int L = slot_len[it];
-    if (L > kListCap) return;
-    int P = 1;
-    while (P < L) P <<= 1;
-    const int* src = pair_node + slot_off[it];
-    __syncthreads();
-    for (int k = t; k < P; k += 64) ids[k] = (k < L) ? src[k] : INT_MAX;
-    __syncthreads();
-    for (int k = 2; k <= P; k <<= 1)
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int a = t; a < P; a += 64) {
-          const int b = a ^ j;
-          if (b > a) {
-            const int va = ids[a], vb = ids[b];
-            const bool up = (a & k) == 0;
-            if ((va > vb) == up) { ids[a] = vb; ids[b] = va; }
-          }
-        }
-        __syncthreads();
-      }
-    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
-    const int x0 = tx * 4, y0 = ty * 4, z0 = tz * 4;
-    const int gx = x0 + (t & 3), gy = y0 + ((t >> 2) & 3), gz = z0 + (t >> 4);
-    const int lane = t & 31;
-    const unsigned* mw = sm.m32[t >> 5];
-    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-    for (int b0 = 0; b0 < L; b0 += 64) {
-      const int nb = min(64, L - b0);
-      if (t < nb) {
-        const long nd = ids[b0 + t];
-        const int sx = st[nd * 3 + 0], sy = st[nd * 3 + 1], sz = st[nd * 3 + 2];
-        s_st[t][0] = sx; s_st[t][1] = sy; s_st[t][2] = sz;
-        for (int a = 0; a < 12; ++a) s_w[t][a] = W[nd * 12 + a];
-        s_fe[t][0] = nodes[nd * 12 + 9]; s_fe[t][1] = nodes[nd * 12 + 10]; s_fe[t][2] = nodes[nd * 12 + 11];
-        const unsigned long long m = stencil_tile_mask(sx - x0, sy - y0, sz - z0);
-        sm.m32[0][t] = (unsigned)m;
-        sm.m32[1][t] = (unsigned)(m >> 32);
-      }
-      __syncthreads();
-      /* node j adds to the cells its stencil covers, in node order; a warp
-         skips the nodes that cover none of its 32 cells (a uniform branch) */
-      for (int j = 0; j < nb; ++j) {
-        const unsigned m = mw[j];
-        if (m == 0u) continue;
-        if ((m >> lane) & 1u) {
-          const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
-          const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
-          Fx = Fx + s_fe[j][0] * tmp;
-          Fy = Fy + s_fe[j][1] * tmp;
-          Fz = Fz + s_fe[j][2] * tmp;
-        }
-      }
-      __syncthreads();
-    }
-    double* Ft = Ftile + (long)it * 192;
-    Ft[t] = Fx; Ft[64 + t] = Fy; Ft[128 + t] = Fz;
-  }
 }
 
 /* Shared memory of one entry-list gather CTA (64 threads = one 4^3 tile):

@@ -63,6 +63,9 @@ def subsample(sheet: np.ndarray) -> np.ndarray:
     return sheet[SUB][:, SUB, :3].reshape(64, 3)
 
 
+AUTOTUNE_MIN_STEPS = 1000
+
+
 def simulate(problems, steps: int, every: int, precision: str, chunk: int = 1024):
     """Run the problems in batches of `chunk`; returns the subsample
     displacement [n, snaps, 64, 3] at t = every, 2 every, ..., steps, the
@@ -77,7 +80,9 @@ def simulate(problems, steps: int, every: int, precision: str, chunk: int = 1024
     for c0 in range(0, n, chunk):
         part = problems[c0:c0 + chunk]
         with lbib.Batch(part, precision, compat=0) as b:
-            if b.variants() > 1:
+            # the kernel-variant trial costs a few dozen steps per size
+            # class: worth it for long runs only
+            if b.variants() > 1 and steps >= AUTOTUNE_MIN_STEPS:
                 b.autotune(4)
             x0 = [subsample(b.sheet(k)) for k in range(len(part))]
             for s in range(snaps):
