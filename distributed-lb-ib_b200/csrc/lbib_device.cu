@@ -589,8 +589,29 @@ static int ensure_scratch(lbib_device* d, long doubles) {
   return 0;
 }
 
+/* The device address of a page-locked host array (cudaHostAlloc /
+ * cudaHostRegister: mapped into the device's address space), or NULL for
+ * pageable memory. */
+static double* mapped_host(double* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return NULL;
+  }
+  return a.type == cudaMemoryTypeHost ? (double*)a.devicePointer : NULL;
+}
+
 extern "C" int lbdev_get_moments(lbib_device* d, double* rho, double* ux, double* uy, double* uz) {
   const long N = d->N;
+  /* page-locked outputs: the moments kernel writes them over the link
+     itself, so nothing is staged in device memory and the copy overlaps
+     the computation */
+  double* m[4] = {mapped_host(rho), mapped_host(ux), mapped_host(uy), mapped_host(uz)};
+  if (m[0] && m[1] && m[2] && m[3]) {
+    if (lbdev_launch_field_moments(d, m[0], m[1], m[2], m[3])) return -2;
+    CK(cudaStreamSynchronize(d->stream));
+    return 0;
+  }
   if (ensure_scratch(d, 4 * N)) return -5;
   double* s = d->scratch;
   if (lbdev_launch_field_moments(d, s, s + N, s + 2 * N, s + 3 * N)) return -2;
