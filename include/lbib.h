@@ -384,7 +384,11 @@ int lbib_load_restart(GV gv, const char* path);
 
 /* Array access for tests, tools and bindings (x-fastest scalar fields,
  * idx = (z*y_dim + y)*x_dim + x; sheet records of 12 doubles in Fibernode
- * order, row-major).  All return LBIB_OK or an error code. */
+ * order, row-major).  All return LBIB_OK or an error code.
+ * lbib_get_moments: when all four outputs are page-locked host memory
+ * (cudaHostAlloc / cudaHostRegister), the moments kernel writes them over
+ * the host link directly; pageable outputs are staged in a device buffer
+ * allocated for the call.  Both give the same values. */
 int lbib_get_moments(GV gv, double* rho, double* ux, double* uy, double* uz);
 int lbib_get_force(GV gv, double* fx, double* fy, double* fz);
 int lbib_get_df1(GV gv, double* out);            /* [19][N], cells of [2,n-3]^3 */
