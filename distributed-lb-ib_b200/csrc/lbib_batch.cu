@@ -23,6 +23,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
+#include <vector>
+
 #include "lbib_batch.cuh"
 #include "lbib_batch_internal.h"
 #include "lbib_ib.cuh"
@@ -185,6 +188,88 @@ int batch_tile_moments_f64(const BatchFluid& f) {
 }  // namespace lbib
 
 /* ------------------------------------------------------------ host state */
+
+
+/* The batch's large buffers (populations, in/outlet tables, force and
+ * moment tiles: hundreds of MB to GBs) come from a small per-process cache:
+ * a buffer freed by one batch is kept (up to a quarter of the device's
+ * memory) and handed to the next batch that fits in it, because releasing
+ * and mapping that much device memory costs tenths of a second per batch
+ * -- a sweep screen that re-runs a few dozen points paid more for its
+ * batch's cudaFree than for its steps.  Every buffer is fully written by
+ * the batch's set-up before use.  A failed allocation empties the cache
+ * and tries again. */
+namespace {
+struct CachedBuf {
+  void* p;
+  size_t n;
+  int dev;
+};
+std::mutex g_cache_mu;
+std::vector<CachedBuf> g_cache;          /* free buffers */
+std::vector<CachedBuf> g_live;           /* buffers handed out */
+size_t g_cached = 0;
+constexpr size_t kCacheMin = (size_t)16 << 20;
+
+void cache_release_all() {
+  for (const CachedBuf& c : g_cache) cudaFree(c.p);
+  g_cache.clear();
+  g_cached = 0;
+}
+
+cudaError_t big_malloc(void** p, size_t n) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  if (n >= kCacheMin) {
+    int best = -1;
+    for (int i = 0; i < (int)g_cache.size(); ++i)
+      if (g_cache[i].dev == dev && g_cache[i].n >= n && g_cache[i].n <= 2 * n &&
+          (best < 0 || g_cache[i].n < g_cache[best].n))
+        best = i;
+    if (best >= 0) {
+      const CachedBuf c = g_cache[best];
+      g_cache.erase(g_cache.begin() + best);
+      g_cached -= c.n;
+      g_live.push_back(c);
+      *p = c.p;
+      return cudaSuccess;
+    }
+  }
+  cudaError_t e = cudaMalloc(p, n);
+  if (e != cudaSuccess && !g_cache.empty()) {
+    cudaGetLastError();
+    cache_release_all();
+    e = cudaMalloc(p, n);
+  }
+  if (e == cudaSuccess) g_live.push_back({*p, n, dev});
+  return e;
+}
+
+void big_free(void* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  for (int i = 0; i < (int)g_live.size(); ++i) {
+    if (g_live[i].p != p) continue;
+    const CachedBuf c = g_live[i];
+    g_live.erase(g_live.begin() + i);
+    size_t fr = 0, total = 0;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(c.dev);
+    cudaMemGetInfo(&fr, &total);
+    cudaSetDevice(cur);
+    if (c.n >= kCacheMin && g_cached + c.n <= total / 4) {
+      g_cache.push_back(c);
+      g_cached += c.n;
+    } else {
+      cudaFree(c.p);
+    }
+    return;
+  }
+  cudaFree(p);
+}
+}  // namespace
 
 #include "../../include/lbib.h"
 
@@ -576,8 +661,8 @@ lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision
   b->CAP = cap;
   b->SP = node0;
   /* pools */
-  if (!rc && cudaMalloc(&b->f, foff) != cudaSuccess) rc = -5;
-  if (!rc && cudaMalloc(&b->tab, toff) != cudaSuccess) rc = -5;
+  if (!rc && big_malloc((void**)&b->f, foff) != cudaSuccess) rc = -5;
+  if (!rc && big_malloc((void**)&b->tab, toff) != cudaSuccess) rc = -5;
   const long NT = b->NT, CAP = b->CAP, SP = b->SP;
   const long nblk = (NT + kScan - 1) / kScan;
   if (!rc && cudaMalloc(&b->tile_cnt, sizeof(int) * NT) != cudaSuccess) rc = -5;
@@ -591,8 +676,8 @@ lbib_batch* lbib_batch_create(int n, const lbib_problem* problems, int precision
     if (cudaMalloc(&b->tile_slot[c], sizeof(int) * NT) != cudaSuccess) rc = -5;
     if (!rc && cudaMalloc(&b->tile_list[c], sizeof(int) * CAP) != cudaSuccess) rc = -5;
     if (!rc && cudaMalloc(&b->tile_count[c], sizeof(int)) != cudaSuccess) rc = -5;
-    if (!rc && cudaMalloc(&b->Ftile[c], sizeof(double) * 192 * CAP) != cudaSuccess) rc = -5;
-    if (!rc && cudaMalloc(&b->Utile[c], sizeof(double) * 256 * CAP) != cudaSuccess) rc = -5;
+    if (!rc && big_malloc((void**)&b->Ftile[c], sizeof(double) * 192 * CAP) != cudaSuccess) rc = -5;
+    if (!rc && big_malloc((void**)&b->Utile[c], sizeof(double) * 256 * CAP) != cudaSuccess) rc = -5;
     if (!rc && cudaMemset(b->tile_count[c], 0, sizeof(int)) != cudaSuccess) rc = -2;
   }
   if (!rc && cudaMalloc(&b->nodes, sizeof(double) * 12 * SP) != cudaSuccess) rc = -5;
@@ -700,12 +785,12 @@ void lbib_batch_free(lbib_batch* b) {
     free(b->sh[k]);
   }
   free(b->sh);
-  cudaFree(b->f); cudaFree(b->tab);
+  big_free(b->f); big_free(b->tab);
   cudaFree(b->tile_cnt); cudaFree(b->tile_inst); cudaFree(b->scan_tmp);
   cudaFree(b->slot_off); cudaFree(b->slot_len); cudaFree(b->slot_cursor); cudaFree(b->pair_node);
   for (int c = 0; c < 2; ++c) {
     cudaFree(b->tile_slot[c]); cudaFree(b->tile_list[c]); cudaFree(b->tile_count[c]);
-    cudaFree(b->Ftile[c]); cudaFree(b->Utile[c]);
+    big_free(b->Ftile[c]); big_free(b->Utile[c]);
     cudaFree(b->P[c]); cudaFree(b->WP[c]);
   }
   cudaFree(b->P_first); cudaFree(b->WP_first);
