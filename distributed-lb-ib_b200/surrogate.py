@@ -28,7 +28,7 @@ sweep is after), or when the members disagree on its tip by more than a
 threshold; every other point is reported from the surrogate: "stops", or
 its tip.  The two thresholds are calibrated on the last eighth of the
 training runs, which the nets do not train on: the loosest settings at which
-98% of the points the surrogate would report there are right.  The judge:
+98% of the points the surrogate would report there are right.  The referee:
 the plain FP64 solver on every point, which the report compares against --
 tip displacement = mean x-displacement of the subsample's last row.
 """
@@ -299,7 +299,7 @@ def pipeline(train_n: int = 4096, eval_n: int = 2048, steps: int = 3000, every: 
     """The whole learned sweep: training runs (batched, FP16 storage), GPU
     training, calibration of the re-run thresholds on the last `calib_frac`
     of the training runs, the plain FP64 batched sweep of the held-out points
-    (the judge, and the baseline rate), and the screen of the same points.
+    (the referee, and the baseline rate), and the screen of the same points.
     With `data`, simulated runs are kept there and reused."""
     import os
     out = {"config": {"train_n": train_n, "eval_n": eval_n, "steps": steps, "every": every, "iters": iters,

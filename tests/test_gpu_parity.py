@@ -7,7 +7,7 @@ Two bars, both stated here:
 * against the reference itself (fixtures from oracle/_ref, which uses the C
   library's cosine, ~0.1% of whose values are 1 ulp off) the relative L2
   error of rho, of u as a vector field and of the fiber positions must be
-  <= 1e-10.
+  <= 1e-10 (the tolerance the drop-in is held to).
 """
 import json
 import os

@@ -54,7 +54,7 @@ def test_surrogate_screen_beats_the_plain_sweep(gpu):
     assert rep["points"] == EVAL and rep["rerun"] + rep["reported_by_surrogate"] == EVAL
     assert rep["rerun"] >= round(0.05 * EVAL)       # the top 5% always go to the solver
     assert rep["rerun"] <= MAX_RERUN * EVAL, rep
-    # the north-star quantity: points/s over the plain FP64 batched sweep, at the 2% bound
+    # the benchmark's quantity: points/s over the plain FP64 batched sweep, at the 2% bound
     assert rep["speedup"] >= MIN_SPEEDUP, rep
     assert rep["right_frac"] >= MIN_RIGHT, rep
     assert rep["rerun_right"] >= 0.9 * rep["rerun"]            # FP16 re-runs judged by FP64

@@ -5,7 +5,7 @@ against the oracle.
   tests/golden/make_golden.py);
 * bit for bit against the reference itself, step by step and stage by
   stage, when oracle/_ref is built (it needs the reference checkout);
-* the correctly-rounded-cosine build stays within the north-star tolerance of
+* the correctly-rounded-cosine build stays within the 1e-10 relative tolerance of
   the reference.
 """
 import os
