@@ -648,7 +648,7 @@ int orc_run(orc_state* s, int nsteps) {
 
 int orc_time(const orc_state* s) { return s->time; }
 
-/* The delta kernel's cosine as this build evaluates it (for tests). */
+/* The delta kernel's cosine as this library variant evaluates it (for tests). */
 double orc_cos(double x) { return ORC_COS(x); }
 
 /* The CUDA path's two-phase form of the same cosine, run on the host (for

@@ -68,7 +68,7 @@ void orc_get_inout(const orc_state* s, int which, double* out);   /* 0 inlet, 1 
 void orc_get_sheet(const orc_state* s, int sheet, double* out);   /* rows*cols*12 */
 void orc_set_sheet(orc_state* s, int sheet, const double* in);
 void orc_set_threads(int n);
-double orc_cos(double x);              /* the delta kernel's cosine of this build */
+double orc_cos(double x);              /* the delta kernel's cosine of this library variant */
 long orc_cos_2phase(const double* x, long n, double* out, unsigned char* slow);  /* the CUDA path's two-phase cosine */
 
 #ifdef __cplusplus
