@@ -251,7 +251,8 @@ extern "C" int lbdev_launch_spread(lbib_device* d, int step) {
   const unsigned nblk = (unsigned)((d->ntiles + kScanBlock - 1) / kScanBlock);
   if (d->scan_state && d->ntiles < (1L << 22) && 8 * S < (1L << 31)) {
     d->scan_tag = d->scan_tag % 255u + 1u;
-    lbib_compact_onepass<<<nblk, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, (int)nblk, d->scan_state, d->scan_tag,
+    const unsigned nb1 = (unsigned)((d->ntiles + kScanBlock * kOnepassTiles - 1) / (kScanBlock * kOnepassTiles));
+    lbib_compact_onepass<<<nb1, kScanBlock, 0, st>>>(d->tile_cnt, d->ntiles, (int)nb1, d->scan_state, d->scan_tag,
                                                       d->tile_list[c], d->tile_slot[c], d->slot_off, d->slot_len,
                                                       d->slot_cursor, d->tile_count[c], d->err);
     d->kernel_launches -= 2;

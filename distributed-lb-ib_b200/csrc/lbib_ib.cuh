@@ -351,6 +351,7 @@ static __global__ void lbib_compact_write(int* __restrict__ cnt, long n, const i
  * then fails) instead of spinning on.  state[nblk] holds the ticket,
  * which the last block resets for the next launch. */
 constexpr long kLookbackSpin = 1L << 22;
+constexpr int kOnepassTiles = 4;   /* tiles per thread: a block covers 4096 tiles */
 constexpr int kErrLookback = -2;   /* the error word's code: LBIB_E_CUDA of include/lbib.h */
 
 __device__ __forceinline__ unsigned long long lookback_word(unsigned tag, unsigned flag, unsigned long long t,
@@ -373,11 +374,18 @@ static __global__ void __launch_bounds__(kScanBlock) lbib_compact_onepass(int* _
   if (threadIdx.x == 0) s_vb = (int)atomicAdd(ticket, 1u);
   __syncthreads();
   const int vb = s_vb;
-  const long i = (long)vb * kScanBlock + threadIdx.x;
-  const int c = (i < n) ? cnt[i] : 0;
-  const int v = c > 0;
+  /* kOnepassTiles consecutive tiles per thread: fewer, fuller blocks, so
+     that every block is resident at once and the look-back walks short */
+  const long i0 = ((long)vb * kScanBlock + threadIdx.x) * kOnepassTiles;
+  int c[kOnepassTiles], tv = 0, tw = 0;
+#pragma unroll
+  for (int k = 0; k < kOnepassTiles; ++k) {
+    c[k] = (i0 + k < n) ? cnt[i0 + k] : 0;
+    tv += c[k] > 0;
+    tw += c[k];
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int iv = v, iw = c;  /* inclusive warp scans */
+  int iv = tv, iw = tw;  /* inclusive warp scans of the threads' totals */
   for (int o = 1; o < 32; o <<= 1) {
     const int tv = __shfl_up_sync(0xffffffffu, iv, o);
     const int tw = __shfl_up_sync(0xffffffffu, iw, o);
@@ -444,17 +452,23 @@ static __global__ void __launch_bounds__(kScanBlock) lbib_compact_onepass(int* _
     }
   }
   __syncthreads();
-  if (v) {
-    const int pos = s_pt + sv[warp] + iv - v;
-    list[pos] = (int)i;
-    slot[i] = pos;
-    slot_off[pos] = s_pp + sw[warp] + iw - c;
-    slot_len[pos] = c;
-    slot_cursor[pos] = 0;
-  } else if (i < n) {
-    slot[i] = -1;     /* the whole map is written: no clearing pass before the step */
+  int pos = s_pt + sv[warp] + iv - tv, off = s_pp + sw[warp] + iw - tw;
+#pragma unroll
+  for (int k = 0; k < kOnepassTiles; ++k) {
+    const long i = i0 + k;
+    if (c[k] > 0) {
+      list[pos] = (int)i;
+      slot[i] = pos;
+      slot_off[pos] = off;
+      slot_len[pos] = c[k];
+      slot_cursor[pos] = 0;
+      cnt[i] = 0;     /* counts start the next step at zero */
+      ++pos;
+      off += c[k];
+    } else if (i < n) {
+      slot[i] = -1;   /* the whole map is written: no clearing pass before the step */
+    }
   }
-  if (i < n && c) cnt[i] = 0;   /* counts start the next step at zero */
 }
 
 /* The one-grid spread's lists hold entries instead of node indices: the
