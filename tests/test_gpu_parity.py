@@ -56,6 +56,10 @@ EXTRA_CASES = {
                                      centred_sheet(40, 16, 16, 8, 4, 0.5, 24.0)]), 15),
     "cube8": (small_case(32, 16, 24, 8, 8, 10.0, cube_size=8), 15),
     "xeqz": (small_case(16, 12, 16, 6, 6, 6.0), 15),
+    # 24 x 16 x 17 = 6,528 tiles: the single-pass compaction runs two blocks of
+    # 4,096 tiles, the second one partial, and the 40 x 40 sheet's stencils
+    # reach tiles on both sides of the block boundary (z 44..47 is tile layer 11)
+    "multiblock": (small_case(96, 64, 68, 40, 40, 20.0), 6),
 }
 
 
