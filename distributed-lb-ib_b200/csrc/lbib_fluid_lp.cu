@@ -17,6 +17,7 @@
 #include <stdlib.h>
 
 #include "lbib_words.cuh"
+#include "lbib_words8.cuh"
 
 extern "C" int lbdev_bulk_rows(const lbib_device* d, int* nrows_y, int* nrows_z);
 
@@ -32,6 +33,18 @@ __global__ void __launch_bounds__(WTPB, MINB) lbib_fluid_step_words(WordsParams<
   /* the plane-adjacent cells x in {2, 3, nx-4, nx-3} of the rows whose first
      word this block holds, while their words are in the caches (their slots
      are theirs alone, so the order within the launch does not matter) */
+  const long r0 = fdiv((unsigned)(first + b.gpr - 1), b.dgpr);
+  long r1 = fdiv((unsigned)(first + WTPB + b.gpr - 1), b.dgpr);
+  if (r1 > b.nrows) r1 = b.nrows;
+  for (long i = threadIdx.x; i < 4 * (r1 - r0); i += WTPB) edge_cell<T, PAR>(b.p, b.nry, (int)(r0 + i / 4), (int)(i & 3));
+}
+
+/* The eight-cell word step (16-bit storage, lbib_words8.cuh), then the
+ * plane-adjacent cells of the rows whose first word this block holds. */
+template <typename T, int PAR, int MINB>
+__global__ void __launch_bounds__(WTPB, MINB) lbib_fluid_step_words8(WordsParams<T> b) {
+  const long first = (long)blockIdx.x * WTPB;
+  words8_item<T, PAR>(b, first + threadIdx.x);
   const long r0 = fdiv((unsigned)(first + b.gpr - 1), b.dgpr);
   long r1 = fdiv((unsigned)(first + WTPB + b.gpr - 1), b.dgpr);
   if (r1 > b.nrows) r1 = b.nrows;
@@ -183,6 +196,33 @@ int launch_words(lbib_device* d, const FluidParamsT<T>& p) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+/* The eight-cell word step (16-bit storage) and the forced cells; the
+ * four-cell kernel where a row is not a whole number of 16-byte words. */
+template <typename T, int MINB>
+int launch_words8(lbib_device* d, const FluidParamsT<T>& p) {
+  if (d->nx % 8) return launch_words<T, 4, MINB>(d, p);
+  WordsParams<T> b;
+  b.p = p;
+  int nry = 0, nrz = 0;
+  if (!lbdev_bulk_rows(d, &nry, &nrz)) return 0;
+  words_geometry(b, 8, d->nx, nry, nrz);
+  const long threads = b.nrows * b.gpr;
+  if (threads + WTPB >= (1L << 31)) return -1;   /* item8 divides 32-bit indices */
+  const unsigned blocks = (unsigned)((threads + WTPB - 1) / WTPB);
+  const int zb = 2 + nrz, c = d->cur;
+  const unsigned fblocks = (unsigned)sm_count() * 8;
+  const bool forced = !p.box;
+  if (d->parity == 0) {
+    lbib_fluid_step_words8<T, 0, MINB><<<blocks, WTPB, 0, d->fluid_stream>>>(b);
+    if (forced) lbib_forced_cells<T, 0><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
+  } else {
+    lbib_fluid_step_words8<T, 1, MINB><<<blocks, WTPB, 0, d->fluid_stream>>>(b);
+    if (forced) lbib_forced_cells<T, 1><<<fblocks, 64, 0, d->stream>>>(p, d->tile_list[c], d->tile_count[c], zb);
+  }
+  d->kernel_launches += forced ? 2 : 1;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 /* The TMA-staged word step (16-bit storage) and the forced cells; the
  * plain word kernel where the row geometry does not suit it. */
 template <typename T, int STAGES, int MINB>
@@ -221,8 +261,15 @@ int launch_words_tma(lbib_device* d, const FluidParamsT<T>& p) {
 }
 
 /* One-grid variants beyond the word-kernel ones of lbib_words.cuh (16-bit
- * storage): {stages, resident CTAs per SM} of the TMA-staged kernel. */
+ * storage): {stages, resident CTAs per SM} of the TMA-staged kernel; the
+ * eight-cell kernel at 4 resident CTAs per SM; and the four-cell {4, 5}
+ * kernel for even steps with that eight-cell one for odd steps.  (The
+ * eight-cell kernel at 3 CTAs per SM, 168 registers, and at 5, 96 registers
+ * with ~450 bytes of spills, measured slower in both parities at
+ * 512x256x256; its odd step gains from the halved shift work per cell, its
+ * even step loses a little to the lower occupancy.) */
 constexpr int kTmaVariants = 3;
+constexpr int kWords8Variants = 2;
 
 /* The box's cells of a box-mode step (after the spread). */
 template <typename T>
@@ -242,6 +289,9 @@ int lp_step(lbib_device* d) {
     if (v == nw) return launch_words_tma<T, 2, 4>(d, p);
     if (v == nw + 1) return launch_words_tma<T, 3, 3>(d, p);
     if (v == nw + 2) return launch_words_tma<T, 2, 5>(d, p);
+    const int v8 = v - nw - kTmaVariants;
+    if (v8 == 0) return launch_words8<T, 4>(d, p);
+    if (v8 == 1) return d->parity == 0 ? launch_words<T, 4, 5>(d, p) : launch_words8<T, 4>(d, p);
   }
   return with_variant<T>(v, [&](auto V, auto MINB) { return launch_words<T, V, MINB>(d, p); });
 }
@@ -314,5 +364,5 @@ extern "C" int lbdev_lp_sums(lbib_device* d, double* part, double* out) {
 /* Word-kernel variants available for a precision (1 for FP64). */
 extern "C" int lbdev_lp_variants(int prec) {
   if (LBIB_PREC_TYPE(prec) == LBIB_PREC_F64) return 1;
-  return word_variants(prec) + (LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? 0 : kTmaVariants);
+  return word_variants(prec) + (LBIB_PREC_TYPE(prec) == LBIB_PREC_F32 ? 0 : kTmaVariants + kWords8Variants);
 }

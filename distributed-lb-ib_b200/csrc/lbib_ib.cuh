@@ -529,20 +529,22 @@ __device__ __forceinline__ unsigned long long stencil_tile_mask(int dx, int dy, 
   return m;
 }
 
+/* A staged node of the entry-list gather: its x, y and z delta weights at
+ * the tile's four cell positions per axis (0 where the stencil misses the
+ * position), then its force.  An odd stride of 15 doubles puts 16
+ * different nodes in 16 different bank pairs. */
+constexpr int kNodeRec = 15;
+
 /* Shared memory of one entry-list gather CTA (64 threads = one 4^3 tile):
  * the list's entries as sort keys (chunk << 32 | lane mask) while the node
- * list is built, then the staged node data while it is summed. */
+ * list is built, then the staged node records while they are summed. */
 struct GatherSmemE {
   int ids[kListCap];                 /* the tile's nodes in index order       */
   int seg[kListCap];                 /* per entry: first node position, or -1 */
   unsigned m32[2][64];               /* per node: the cells of warp 0 / 1     */
   union {
     unsigned long long key[kListCap];
-    struct {
-      int st[64][3];
-      double w[64][12];
-      double fe[64][3];
-    } n;
+    double rec[64 * kNodeRec];
   } u;
 };
 
@@ -605,13 +607,12 @@ __device__ __forceinline__ void gather_tile_ent(GatherSmemE& sm, const double* _
     const int base = (int)(key[e] >> 32) * 32;
     for (unsigned m = (unsigned)key[e]; m; m &= m - 1) sm.ids[pos++] = base + __ffs(m) - 1;
   }
-  __syncthreads();   /* ids complete; key no longer read (aliases the node data) */
-  auto& s_st = sm.u.n.st;
-  auto& s_w = sm.u.n.w;
-  auto& s_fe = sm.u.n.fe;
+  __syncthreads();   /* ids complete; key no longer read (aliases the node records) */
+  double* rec = sm.u.rec;
   const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
   const int x0 = tx * 4, y0 = ty * 4, z0 = tz * 4;
-  const int gx = x0 + (t & 3), gy = y0 + ((t >> 2) & 3), gz = z0 + (t >> 4);
+  /* the thread's cell in a record: its x, y and z weight positions */
+  const int ox = t & 3, oy = 4 + ((t >> 2) & 3), oz = 8 + (t >> 4);
   const int lane = t & 31;
   const unsigned* mw = sm.m32[t >> 5];
   double Fx = 0.0, Fy = 0.0, Fz = 0.0;
@@ -620,9 +621,17 @@ __device__ __forceinline__ void gather_tile_ent(GatherSmemE& sm, const double* _
     if (t < nb) {
       const long nd = sm.ids[b0 + t];
       const int sx = st[nd * 3 + 0], sy = st[nd * 3 + 1], sz = st[nd * 3 + 2];
-      s_st[t][0] = sx; s_st[t][1] = sy; s_st[t][2] = sz;
-      for (int a = 0; a < 12; ++a) s_w[t][a] = W[nd * 12 + a];
-      s_fe[t][0] = nodes[nd * 12 + 9]; s_fe[t][1] = nodes[nd * 12 + 10]; s_fe[t][2] = nodes[nd * 12 + 11];
+      double* r = rec + t * kNodeRec;
+      const double* w = W + nd * 12;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        /* cell position c of the tile is stencil position c + (x0 - sx) */
+        const int a = c + x0 - sx, b = c + y0 - sy, e = c + z0 - sz;
+        r[c] = (unsigned)a < 4u ? w[a] : 0.0;
+        r[4 + c] = (unsigned)b < 4u ? w[4 + b] : 0.0;
+        r[8 + c] = (unsigned)e < 4u ? w[8 + e] : 0.0;
+      }
+      r[12] = nodes[nd * 12 + 9]; r[13] = nodes[nd * 12 + 10]; r[14] = nodes[nd * 12 + 11];
       const unsigned long long m = stencil_tile_mask(sx - x0, sy - y0, sz - z0);
       sm.m32[0][t] = (unsigned)m;
       sm.m32[1][t] = (unsigned)(m >> 32);
@@ -641,12 +650,11 @@ __device__ __forceinline__ void gather_tile_ent(GatherSmemE& sm, const double* _
         x = (lane & k) ? (x & ~M) | ((y & ~M) >> k) : (x & M) | ((y & M) << k);
       }
       for (unsigned bits = x; bits; bits &= bits - 1u) {
-        const int j = j0 + __ffs(bits) - 1;
-        const int a = gx - s_st[j][0], b = gy - s_st[j][1], e = gz - s_st[j][2];
-        const double tmp = cf * s_w[j][a] * s_w[j][4 + b] * s_w[j][8 + e];
-        Fx = Fx + s_fe[j][0] * tmp;
-        Fy = Fy + s_fe[j][1] * tmp;
-        Fz = Fz + s_fe[j][2] * tmp;
+        const double* r = rec + (j0 + __ffs(bits) - 1) * kNodeRec;
+        const double tmp = cf * r[ox] * r[oy] * r[oz];
+        Fx = Fx + r[12] * tmp;
+        Fy = Fy + r[13] * tmp;
+        Fz = Fz + r[14] * tmp;
       }
     }
     __syncthreads();

@@ -82,11 +82,19 @@ struct Word {
   uint32_t r[NR];
 
   __device__ __forceinline__ void load(const U* a) {
-    if constexpr (NR == 2) { const uint2 v = *reinterpret_cast<const uint2*>(a); r[0] = v.x; r[1] = v.y; }
-    else r[0] = *reinterpret_cast<const uint32_t*>(a);
+    if constexpr (NR == 4) {
+      const uint4 v = *reinterpret_cast<const uint4*>(a);
+      r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = v.w;
+    } else if constexpr (NR == 2) {
+      const uint2 v = *reinterpret_cast<const uint2*>(a);
+      r[0] = v.x; r[1] = v.y;
+    } else {
+      r[0] = *reinterpret_cast<const uint32_t*>(a);
+    }
   }
   __device__ __forceinline__ void store(U* a) const {
-    if constexpr (NR == 2) *reinterpret_cast<uint2*>(a) = make_uint2(r[0], r[1]);
+    if constexpr (NR == 4) *reinterpret_cast<uint4*>(a) = make_uint4(r[0], r[1], r[2], r[3]);
+    else if constexpr (NR == 2) *reinterpret_cast<uint2*>(a) = make_uint2(r[0], r[1]);
     else *reinterpret_cast<uint32_t*>(a) = r[0];
   }
   __device__ __forceinline__ void clear() {
