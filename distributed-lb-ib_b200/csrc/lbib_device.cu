@@ -531,6 +531,8 @@ extern "C" int lbdev_step(lbib_device* d, int step_no) {
 }
 
 extern "C" int lbdev_profile_begin(lbib_device* d) {
+  /* the first events are made here, not inside the profiled steps */
+  if (!d->prof_cap && prof_grow(d)) return -5;
   d->profiling = 1;
   d->prof_steps = 0;
   return 0;
