@@ -58,13 +58,26 @@ __device__ __forceinline__ void x2_relax_cell(const FluidParams& p, int x, int y
   }
 }
 
-/* One cell's loads through the generic rules (plane cells). */
-template <int PAR>
-__device__ __forceinline__ void x2_load_one(const FluidParams& p, int x, int y, int z, long idx, double f[19]) {
-  load_pre<PAR>(p, x, y, z, idx, (x == 2 || x == p.nx - 3) ? K_TABLE : K_FAST, f);
+/* The plane cell of a pair (x = 2: the inlet, x = nx-3: the outlet) takes
+ * its populations from the fixed table (load_pre's K_TABLE rule); rows of
+ * this kernel have z <= zin_hi, where every plane cell is a table cell. */
+__device__ __forceinline__ void x2_plane_table(const FluidParams& p, int y, int z, bool pa, double fa[19],
+                                               double fb[19]) {
+  const double* t = pa ? p.inlet : p.outlet;
+  const long P = (long)p.ny * p.nz, pi = (long)y * p.nz + z;
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    const double v = t[q * P + pi];
+    if (pa) fa[q] = v; else fb[q] = v;
+  }
 }
 
-/* The step of the pair (x, x+1) of row (y, z); x even. */
+/* The step of the pair (x, x+1) of row (y, z); x even.  A pair holding a
+ * plane cell runs the same loads and stores as every other pair -- the
+ * plane cell's pulled values are then replaced by its table, and in an odd
+ * step its pushes that would leave I (c_x = -1 at x = 2, +1 at x = nx-3) go
+ * to its own slot opp(q) by an address select, store_post's rule -- so the
+ * warp holding it does not diverge into the per-cell rules. */
 template <int PAR>
 __device__ __forceinline__ void x2_pair(const FluidParams& p, int x, int y, int z) {
   if (p.box && in_box(p.box, x, y, z)) return;    /* both cells share a tile (x even) */
@@ -73,38 +86,39 @@ __device__ __forceinline__ void x2_pair(const FluidParams& p, int x, int y, int 
   double* __restrict__ F = p.f;
   double fa[19], fb[19];
   double* __restrict__ Fi = F + idx;
-  if (!pa && !pb) {
 #pragma unroll
-    for (int q = 0; q < 19; ++q) {
-      if (PAR == 0 || cx(q) == 0) {
-        const double* src = PAR ? Fi + p.pull[q] : Fi + q * p.N;
-        const double2 v = *reinterpret_cast<const double2*>(src);
-        fa[q] = v.x; fb[q] = v.y;
-      } else {
-        const double* src = Fi + p.pull[q];
-        fa[q] = src[0]; fb[q] = src[1];
-      }
+  for (int q = 0; q < 19; ++q) {
+    if (PAR == 0 || cx(q) == 0) {
+      const double* src = PAR ? Fi + p.pull[q] : Fi + q * p.N;
+      const double2 v = *reinterpret_cast<const double2*>(src);
+      fa[q] = v.x; fb[q] = v.y;
+    } else {
+      const double* src = Fi + p.pull[q];
+      fa[q] = src[0]; fb[q] = src[1];
     }
-  } else {
-    x2_load_one<PAR>(p, x, y, z, idx, fa);
-    x2_load_one<PAR>(p, x + 1, y, z, idx + 1, fb);
   }
+  if (pa || pb) x2_plane_table(p, y, z, pa, fa, fb);
   x2_relax_cell(p, x, y, z, pa, fa);
   x2_relax_cell(p, x + 1, y, z, pb, fb);
   if (PAR == 0) {
 #pragma unroll
     for (int q = 0; q < 19; ++q)
       *reinterpret_cast<double2*>(Fi + opp(q) * p.N) = make_double2(fa[q], fb[q]);
-  } else if (!pa && !pb) {
+  } else {
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
       double* dst = Fi + p.push[q];
-      if (cx(q) == 0) *reinterpret_cast<double2*>(dst) = make_double2(fa[q], fb[q]);
-      else { dst[0] = fa[q]; dst[1] = fb[q]; }
+      if (cx(q) == 0) {
+        *reinterpret_cast<double2*>(dst) = make_double2(fa[q], fb[q]);
+      } else {
+        double* da = dst;
+        double* db = dst + 1;
+        if (cx(q) == -1) da = pa ? Fi + opp(q) * p.N : da;
+        else db = pb ? Fi + 1 + opp(q) * p.N : db;
+        *da = fa[q];
+        *db = fb[q];
+      }
     }
-  } else {
-    store_post<PAR>(p, x, y, z, idx, pa ? K_TABLE : K_FAST, fa);
-    store_post<PAR>(p, x + 1, y, z, idx + 1, pb ? K_TABLE : K_FAST, fb);
   }
 }
 
