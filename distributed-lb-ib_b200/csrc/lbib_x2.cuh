@@ -72,12 +72,14 @@ __device__ __forceinline__ void x2_plane_table(const FluidParams& p, int y, int 
   }
 }
 
-/* The step of the pair (x, x+1) of row (y, z); x even.  A pair holding a
- * plane cell runs the same loads and stores as every other pair -- the
- * plane cell's pulled values are then replaced by its table, and in an odd
- * step its pushes that would leave I (c_x = -1 at x = 2, +1 at x = nx-3) go
- * to its own slot opp(q) by an address select, store_post's rule -- so the
- * warp holding it does not diverge into the per-cell rules. */
+/* The step of the pair (x, x+1) of row (y, z); x even.  In an odd step a
+ * pair holding a plane cell runs the same loads and stores as every other
+ * pair -- the plane cell's pulled values are then replaced by its table, and
+ * its pushes that would leave I (c_x = -1 at x = 2, +1 at x = nx-3) go to
+ * its own slot opp(q) by an address select, store_post's rule -- so the warp
+ * holding it does not diverge into the per-cell rules (1.89 -> 1.79 ms per
+ * FP64 step at 512x256x256).  Its even-step loads keep the per-cell rules,
+ * which measured faster there (even-step fluid 1.75 -> 1.67 ms). */
 template <int PAR>
 __device__ __forceinline__ void x2_pair(const FluidParams& p, int x, int y, int z) {
   if (p.box && in_box(p.box, x, y, z)) return;    /* both cells share a tile (x even) */
@@ -86,18 +88,24 @@ __device__ __forceinline__ void x2_pair(const FluidParams& p, int x, int y, int 
   double* __restrict__ F = p.f;
   double fa[19], fb[19];
   double* __restrict__ Fi = F + idx;
+  if (PAR == 0 && (pa || pb)) {
+    /* even step: the per-cell rules (own slots; the plane cell's table) */
+    load_pre<PAR>(p, x, y, z, idx, pa ? K_TABLE : K_FAST, fa);
+    load_pre<PAR>(p, x + 1, y, z, idx + 1, pb ? K_TABLE : K_FAST, fb);
+  } else {
 #pragma unroll
-  for (int q = 0; q < 19; ++q) {
-    if (PAR == 0 || cx(q) == 0) {
-      const double* src = PAR ? Fi + p.pull[q] : Fi + q * p.N;
-      const double2 v = *reinterpret_cast<const double2*>(src);
-      fa[q] = v.x; fb[q] = v.y;
-    } else {
-      const double* src = Fi + p.pull[q];
-      fa[q] = src[0]; fb[q] = src[1];
+    for (int q = 0; q < 19; ++q) {
+      if (PAR == 0 || cx(q) == 0) {
+        const double* src = PAR ? Fi + p.pull[q] : Fi + q * p.N;
+        const double2 v = *reinterpret_cast<const double2*>(src);
+        fa[q] = v.x; fb[q] = v.y;
+      } else {
+        const double* src = Fi + p.pull[q];
+        fa[q] = src[0]; fb[q] = src[1];
+      }
     }
+    if (pa || pb) x2_plane_table(p, y, z, pa, fa, fb);
   }
-  if (pa || pb) x2_plane_table(p, y, z, pa, fa, fb);
   x2_relax_cell(p, x, y, z, pa, fa);
   x2_relax_cell(p, x + 1, y, z, pb, fb);
   if (PAR == 0) {
